@@ -1,0 +1,200 @@
+/*
+ * interflect-b200 C ABI: the stage API of Interflect's surfel-radiosity path
+ * (scene -> surfels -> transfer -> solve -> shade), executed on one NVIDIA
+ * B200 (sm_100a) by hand-written CUDA kernels.
+ *
+ * The reference crate (`interflect` 0.1.3, Rust) has no FFI: its stages are
+ * crate-internal functions called from src/main.rs. Each entry point below
+ * replaces one of those functions; the citation names the reference function
+ * (file:line, relative to the crate root) whose behaviour it reproduces. A
+ * Rust host binds these with `extern "C"` declarations.
+ *
+ * Conventions
+ *  - Every function returns an int status: IFX_OK (0) or an IFX_ERR_* code.
+ *    On error the context's message is available from ifx_last_error().
+ *    No C++ exception crosses this boundary.
+ *  - Vectors are packed f32 triples (x, y, z) in caller-owned host memory.
+ *    Output pointers documented as nullable may be NULL to skip that copy.
+ *  - Device state (scene, surfels, transfer matrix, grid, film) is owned by
+ *    the context. A context drives one GPU on one CUDA stream; it is not
+ *    thread-safe, but separate contexts are independent.
+ *  - There is no CPU fallback: without a usable CUDA device every
+ *    device-side call fails with IFX_ERR_CUDA.
+ *  - Results are deterministic: bit-identical across runs and launch
+ *    configurations (no floating-point atomics; every float reduction runs
+ *    in a fixed order).
+ */
+#ifndef INTERFLECT_H
+#define INTERFLECT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IFX_OK 0
+#define IFX_ERR_INVALID 1  /* bad argument or call order */
+#define IFX_ERR_PARSE 2    /* malformed .rad scene (scene.rs:365-571 errors) */
+#define IFX_ERR_CUDA 3     /* CUDA runtime failure or no device */
+#define IFX_ERR_NOMEM 4    /* device or host allocation failed */
+#define IFX_ERR_LIMIT 5    /* a size limit was exceeded */
+#define IFX_ERR_TIMEOUT 6  /* a bounded device-side wait expired */
+
+/* Render modes: main.rs:25-39 (the path-traced `reference` mode is not part
+ * of this library). */
+#define IFX_MODE_BEAUTY 0
+#define IFX_MODE_DIRECT 1
+#define IFX_MODE_INDIRECT 2
+#define IFX_MODE_NORMALS 3
+#define IFX_MODE_DEPTH 4
+#define IFX_MODE_STEPS 5
+
+typedef struct ifx_scene ifx_scene; /* host-side parsed scene */
+typedef struct ifx_ctx ifx_ctx;     /* one GPU, one stream */
+
+/* scene.rs:78-84 RenderCfg */
+typedef struct ifx_render_cfg {
+    uint32_t width, height;
+    uint64_t surfels;
+    uint32_t bounces;
+    float exposure;
+} ifx_render_cfg;
+
+/* scene.rs:59-64 Camera */
+typedef struct ifx_camera {
+    float pos[3], look[3], up[3];
+    float fov; /* degrees */
+} ifx_camera;
+
+typedef struct ifx_scene_info {
+    uint32_t objects;     /* bounded objects (BVH) */
+    uint32_t planes;      /* unbounded objects */
+    uint32_t lights;      /* quad lights */
+    uint32_t sphere_lights;
+    uint32_t materials;   /* excluding the implicit default material */
+    uint32_t bvh_nodes;
+    float bounds_lo[3], bounds_hi[3]; /* scene.rs:573-601 world_bounds */
+    ifx_render_cfg cfg;
+    ifx_camera camera;
+} ifx_scene_info;
+
+/* formfactor.rs:48-66 Transfer (scalars) plus the evaluation count that
+ * formfactor::build returns. */
+typedef struct ifx_transfer_info {
+    uint64_t clusters;
+    uint64_t links;
+    uint64_t candidates;  /* pairs that reached the visibility trace */
+    uint64_t evals;       /* SDF evaluations, reference counting rule */
+    uint64_t interior_rows;
+    float mean_row_sum;
+} ifx_transfer_info;
+
+/* solve.rs:102-105 SolveStats */
+typedef struct ifx_solve_stats {
+    uint32_t iterations;
+    float residual;
+} ifx_solve_stats;
+
+/* Device timing and launch accounting of the most recent calls. */
+typedef struct ifx_stats {
+    uint64_t kernel_launches;  /* kernels this context has launched so far */
+    float ms_transfer, ms_light, ms_solve, ms_grid, ms_shade; /* CUDA-event times of the last call of each stage */
+} ifx_stats;
+
+/* ------------------------------------------------------------- scene --- */
+
+/* Parses a .rad scene and builds its BVH on the host.
+ * Replaces scene::parse (src/scene.rs:365-571) and Bvh::build
+ * (src/bvh.rs:53-91). On IFX_ERR_PARSE, `err` receives the diagnostic the
+ * reference would print after "error: " (truncated to errlen). */
+int ifx_scene_parse(const char* src, size_t len, ifx_scene** out, char* err, size_t errlen);
+void ifx_scene_free(ifx_scene* scene);
+int ifx_scene_get_info(const ifx_scene* scene, ifx_scene_info* out);
+/* Applies CLI overrides and re-validates them, as main.rs:394-413 does with
+ * RenderCfg::validate (src/scene.rs:106-148). The message goes to `err`. */
+int ifx_scene_set_cfg(ifx_scene* scene, const ifx_render_cfg* cfg, char* err, size_t errlen);
+/* --no-bvh: linear object scan instead of the BVH (scene.rs:202-206). */
+int ifx_scene_set_use_bvh(ifx_scene* scene, int use_bvh);
+/* The host-built BVH (bvh.rs:27-36 node fields): per node lo(3) hi(3) as
+ * f32 then start, count, right as u32 (9 words), and the leaf object order
+ * (one u32 per bounded object). Both pointers nullable. */
+int ifx_scene_get_bvh(const ifx_scene* scene, uint32_t* nodes9, uint32_t* order);
+
+/* ----------------------------------------------------------- context --- */
+
+int ifx_ctx_create(int device, ifx_ctx** out);
+void ifx_ctx_destroy(ifx_ctx* ctx);
+const char* ifx_last_error(const ifx_ctx* ctx);
+int ifx_get_stats(const ifx_ctx* ctx, ifx_stats* out);
+
+/* Flattens the scene (SDF object program, BVH nodes, planes, lights,
+ * materials) into device memory. Must precede every stage below. */
+int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene);
+
+/* ----------------------------------------------------------- surfels --- */
+
+/* Replaces surfel::generate (src/surfel.rs:147-255): Halton seeds projected
+ * onto the SDF on the GPU, then Poisson-thinned in seed order on the host.
+ * `placed` receives the surfel count. */
+int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* placed);
+
+/* Installs caller-provided surfels (src/surfel.rs:23-38 fields p, n, albedo,
+ * area); direct/irr/rad start at zero. */
+int ifx_surfels_upload(ifx_ctx* ctx, uint64_t n, const float* p, const float* nrm, const float* albedo,
+                       const float* area);
+int ifx_surfels_count(const ifx_ctx* ctx, uint64_t* n);
+/* Copies surfel state out. Every pointer is nullable. */
+int ifx_surfels_download(ifx_ctx* ctx, float* p, float* nrm, float* albedo, float* area, float* direct,
+                         float* irr, float* rad);
+
+/* ---------------------------------------------------------- transfer --- */
+
+/* Replaces formfactor::build_clusters (src/formfactor.rs:91-147) followed by
+ * formfactor::build (src/formfactor.rs:153-277): clusters, candidate pairs,
+ * cone-traced visibility, hemisphere-closure calibration and the CSR matrix,
+ * all on the GPU. */
+int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out);
+/* CSR arrays: starts (n+1), idx (links), w (links). Nullable. */
+int ifx_transfer_download(ifx_ctx* ctx, uint32_t* starts, uint32_t* idx, float* w);
+/* Clusters: per cluster p(3) n(3) area radius; member offsets (nc+1) and the
+ * member list (n). Nullable. */
+int ifx_clusters_download(ifx_ctx* ctx, float* pnar8, uint32_t* offsets, uint32_t* members);
+/* Per-row diagnostics: calibrated row sum (min 1), sky fraction, SDF
+ * evaluations, candidate pairs. Nullable. */
+int ifx_transfer_row_diag(ifx_ctx* ctx, float* row_sum, float* row_sky, uint64_t* row_evals,
+                          uint32_t* cand_count);
+/* Installs a caller-provided CSR matrix over the current clusters. */
+int ifx_transfer_upload(ifx_ctx* ctx, const uint32_t* starts, uint64_t links, const uint32_t* idx,
+                        const float* w);
+
+/* ------------------------------------------------------------- solve --- */
+
+/* Replaces solve::light_surfels (src/solve.rs:27-39): direct diffuse light
+ * (E) on every surfel; sets direct = rad = E and irr = 0. */
+int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals);
+
+/* Replaces solve::solve (src/solve.rs:47-108): Jacobi bounces with
+ * area-weighted cluster aggregation, until the residual drops below 1e-4 or
+ * max_bounces is reached. */
+int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* out);
+
+/* ------------------------------------------------------------- shade --- */
+
+/* Replaces surfel::Grid::build (src/surfel.rs:71-114) with the gather radius
+ * main.rs:473-475 uses. radius <= 0 selects diag/sqrt(cfg.surfels)*2.6. */
+int ifx_grid_build(ifx_ctx* ctx, float radius);
+
+/* Replaces render_frame (src/main.rs:229-367) followed by Film::encode
+ * (src/film.rs:51-61). `cam` NULL uses the scene camera. out_linear
+ * (w*h*3 f32, row-major) and out_srgb (w*h*3 u8) are nullable host buffers.
+ * `evals` receives the SDF evaluation count (nullable). */
+int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
+                     float* out_linear, uint8_t* out_srgb, uint64_t* evals);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* INTERFLECT_H */

@@ -1,0 +1,98 @@
+"""Builds the native parts of interflect_b200 in-tree.
+
+Outputs
+  interflect_b200/lib/libinterflect_b200.so   CUDA kernels + C ABI (sm_100a)
+  interflect_b200/bin/interflect              the `interflect render` CLI
+
+The kernels are compiled with --fmad=false and IEEE division and square
+root so that every f32 expression rounds exactly as the reference's unfused
+arithmetic does; host code that computes values the device reuses is built
+with -ffp-contract=off for the same reason.
+
+Usage: python -m interflect_b200.build [--force] [--verbose]
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "lib", "libinterflect_b200.so")
+CLI = os.path.join(HERE, "bin", "interflect")
+
+CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "capi.cu"]
+CPP_SOURCES = ["scene_host.cpp"]
+HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
+              "-ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I", os.path.join(ROOT, "include")]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wextra",
+             "-Wno-unused-parameter"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found: the CUDA toolkit is required to build interflect_b200")
+
+
+def cuda_root() -> str:
+    return os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd: list[str], verbose: bool) -> None:
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=not verbose, text=True)
+    if r.returncode != 0:
+        out = (r.stdout or "") + (r.stderr or "")
+        raise RuntimeError(f"build step failed ({r.returncode}): {' '.join(cmd)}\n{out}")
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "interflect.h")]
+    objs = []
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs + [__file__]):
+            _run([nvcc(), *ARCH, *NVCC_FLAGS, "-c", s, "-o", o], verbose)
+    for src in CPP_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs + [__file__]):
+            _run(["g++", *CXX_FLAGS, "-c", s, "-o", o], verbose)
+    cudalib = os.path.join(cuda_root(), "lib64")
+    if force or _stale(LIB, objs):
+        _run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-L", cudalib, "-lcudart_static", "-lpthread", "-ldl",
+              "-lrt"], verbose)
+    cli_src = os.path.join(CSRC, "cli.cpp")
+    png_src = os.path.join(CSRC, "png.cpp")
+    if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, png_src, LIB] + hdrs)):
+        _run(["g++", *CXX_FLAGS, "-I", os.path.join(ROOT, "include"), cli_src, png_src, "-o", CLI,
+              "-L", os.path.dirname(LIB), "-linterflect_b200", "-Wl,-rpath,$ORIGIN/../lib", "-lz"], verbose)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
+    print(LIB)

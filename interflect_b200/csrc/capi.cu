@@ -1,0 +1,973 @@
+// C ABI (include/interflect.h): context, device memory and stage sequencing.
+#include <cub/cub.cuh>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/interflect.h"
+#include "kernels.h"
+#include "scene_host.h"
+
+using namespace ifx;
+
+struct ifx_scene {
+    HScene s;
+};
+
+namespace {
+
+struct DBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+// Largest program blob staged into shared memory; bigger scenes are read
+// from global memory through the read-only cache.
+const uint32_t kMaxStagedBlob = 96 * 1024;
+
+}  // namespace
+
+struct ifx_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+    ifx_stats stats{};
+
+    // scene
+    bool has_scene = false;
+    HScene scene;
+    DBuf blob;
+    BlobRef blobref{};
+    SceneConsts sc{};
+    DBuf status;  // uint32 device status word
+    DBuf srgb_t;  // 256 f32 thresholds
+
+    // surfels
+    uint32_t n = 0;
+    DBuf sp, sn, salb, sdir, sirr, srad;
+
+    // clusters
+    uint32_t nc = 0, nseg = 0;
+    DBuf keys, keys_alt, heads, head_scan, seg_start, members, cp_tmp, cn_tmp, valid, valid_scan, cp, cn, crange;
+
+    // transfer
+    bool has_transfer = false;
+    uint64_t ncand = 0, links = 0;
+    DBuf cand_count, cand_off, cand_c, cand_ff, cand_row, cand_vis, cand_steps;
+    DBuf row_open, row_csteps, row_links, row_scale, row_sum, row_sky, row_evals, starts, idx, w;
+
+    // solve
+    DBuf cluster_rad, ctl;
+
+    // grid
+    bool has_grid = false;
+    GridParams grid{};
+    uint32_t ncells = 0;
+    DBuf gkeys, gkeys_alt, gstarts, gp, gn, girr, gitems;
+
+    // film
+    DBuf film, out8;
+
+    // scratch
+    DBuf cub_tmp, small;  // small: 8 x u64 counters / results
+    DBuf gen_cand;
+    std::vector<float4> gen_host;
+
+    SurfelArrays sarr() {
+        return SurfelArrays{(float4*)sp.p, (float4*)sn.p, (float4*)salb.p, (float4*)sdir.p, (float4*)sirr.p,
+                            (float4*)srad.p};
+    }
+};
+
+// ------------------------------------------------------------ helpers ----
+static int fail(ifx_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(ctx, IFX_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+#define CKL()                                                                                          \
+    do {                                                                                               \
+        cudaError_t e_ = cudaGetLastError();                                                           \
+        if (e_ != cudaSuccess) return fail(ctx, IFX_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+static int ensure(ifx_ctx* ctx, DBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return IFX_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, IFX_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                                            cudaGetErrorString(e));
+    }
+    b.cap = bytes;
+    return IFX_OK;
+}
+
+#define ENSURE(buf, bytes)                             \
+    do {                                               \
+        int r_ = ensure(ctx, (buf), (size_t)(bytes));  \
+        if (r_ != IFX_OK) return r_;                   \
+    } while (0)
+
+static void free_buf(DBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+}
+
+// Reads and clears the device status word; a set bit means a bounded wait
+// expired inside a kernel.
+static int check_status(ifx_ctx* ctx) {
+    uint32_t s = 0;
+    CK(cudaMemcpyAsync(&s, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (s) {
+        CK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->st));
+        return fail(ctx, IFX_ERR_TIMEOUT, "a device-side bounded wait expired (status 0x" + std::to_string(s) + ")");
+    }
+    return IFX_OK;
+}
+
+template <class F>
+static int cub_call(ifx_ctx* ctx, F f) {
+    size_t bytes = 0;
+    CK(f(nullptr, bytes));
+    ENSURE(ctx->cub_tmp, bytes);
+    size_t have = ctx->cub_tmp.cap;
+    CK(f(ctx->cub_tmp.p, have));
+    ctx->launches += 2;
+    return IFX_OK;
+}
+
+#define CUB(expr)                             \
+    do {                                      \
+        int r_ = cub_call(ctx, expr);         \
+        if (r_ != IFX_OK) return r_;          \
+    } while (0)
+
+static void copy_err(const std::string& m, char* err, size_t errlen) {
+    if (!err || errlen == 0) return;
+    size_t k = m.size() < errlen - 1 ? m.size() : errlen - 1;
+    memcpy(err, m.data(), k);
+    err[k] = '\0';
+}
+
+// --------------------------------------------------------------- scene ---
+extern "C" int ifx_scene_parse(const char* src, size_t len, ifx_scene** out, char* err, size_t errlen) {
+    if (!src || !out) return IFX_ERR_INVALID;
+    *out = nullptr;
+    ifx_scene* s = new (std::nothrow) ifx_scene();
+    if (!s) return IFX_ERR_NOMEM;
+    std::string e;
+    if (!parse_rad(std::string(src, len), s->s, e)) {
+        copy_err(e, err, errlen);
+        delete s;
+        return IFX_ERR_PARSE;
+    }
+    *out = s;
+    return IFX_OK;
+}
+
+extern "C" void ifx_scene_free(ifx_scene* s) { delete s; }
+
+extern "C" int ifx_scene_get_info(const ifx_scene* scene, ifx_scene_info* out) {
+    if (!scene || !out) return IFX_ERR_INVALID;
+    const HScene& s = scene->s;
+    memset(out, 0, sizeof *out);
+    out->objects = (uint32_t)s.objects.size();
+    out->planes = (uint32_t)s.planes.size();
+    out->lights = (uint32_t)s.lights.size();
+    out->sphere_lights = (uint32_t)s.sphere_lights.size();
+    out->materials = (uint32_t)s.materials.size() - 1;
+    out->bvh_nodes = (uint32_t)s.nodes.size();
+    out->bounds_lo[0] = s.lo.x; out->bounds_lo[1] = s.lo.y; out->bounds_lo[2] = s.lo.z;
+    out->bounds_hi[0] = s.hi.x; out->bounds_hi[1] = s.hi.y; out->bounds_hi[2] = s.hi.z;
+    out->cfg.width = s.cfg.width;
+    out->cfg.height = s.cfg.height;
+    out->cfg.surfels = s.cfg.surfels;
+    out->cfg.bounces = s.cfg.bounces;
+    out->cfg.exposure = s.cfg.exposure;
+    const HCamera& c = s.camera;
+    out->camera.pos[0] = c.pos.x; out->camera.pos[1] = c.pos.y; out->camera.pos[2] = c.pos.z;
+    out->camera.look[0] = c.look.x; out->camera.look[1] = c.look.y; out->camera.look[2] = c.look.z;
+    out->camera.up[0] = c.up.x; out->camera.up[1] = c.up.y; out->camera.up[2] = c.up.z;
+    out->camera.fov = c.fov;
+    return IFX_OK;
+}
+
+extern "C" int ifx_scene_set_cfg(ifx_scene* scene, const ifx_render_cfg* cfg, char* err, size_t errlen) {
+    if (!scene || !cfg) return IFX_ERR_INVALID;
+    HCfg h;
+    h.width = cfg->width;
+    h.height = cfg->height;
+    h.surfels = cfg->surfels;
+    h.bounces = cfg->bounces;
+    h.exposure = cfg->exposure;
+    std::string e;
+    if (!validate_cfg(h, e)) {
+        copy_err(e, err, errlen);
+        return IFX_ERR_LIMIT;
+    }
+    scene->s.cfg = h;
+    return IFX_OK;
+}
+
+extern "C" int ifx_scene_get_bvh(const ifx_scene* scene, uint32_t* nodes9, uint32_t* order) {
+    if (!scene) return IFX_ERR_INVALID;
+    const HScene& s = scene->s;
+    for (size_t i = 0; nodes9 && i < s.nodes.size(); ++i) {
+        const DNode& n = s.nodes[i];
+        uint32_t* d = nodes9 + 9 * i;
+        memcpy(d, n.lo, 12);
+        memcpy(d + 3, n.hi, 12);
+        d[6] = n.count > 0 ? (uint32_t)n.link : 0u;
+        d[7] = (uint32_t)n.count;
+        d[8] = n.count > 0 ? 0u : (uint32_t)n.link;
+    }
+    for (size_t i = 0; order && i < s.order.size(); ++i) order[i] = s.order[i];
+    return IFX_OK;
+}
+
+extern "C" int ifx_scene_set_use_bvh(ifx_scene* scene, int use_bvh) {
+    if (!scene) return IFX_ERR_INVALID;
+    scene->s.use_bvh = use_bvh != 0;
+    return IFX_OK;
+}
+
+// ------------------------------------------------------------- context ---
+extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
+    if (!out) return IFX_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return IFX_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return IFX_ERR_INVALID;
+    ifx_ctx* ctx = new (std::nothrow) ifx_ctx();
+    if (!ctx) return IFX_ERR_NOMEM;
+    ctx->device = device;
+    auto bail = [&](cudaError_t er) {
+        (void)er;
+        delete ctx;
+        return IFX_ERR_CUDA;
+    };
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) return bail(e);
+    if (ensure(ctx, ctx->status, 16) != IFX_OK || ensure(ctx, ctx->small, 64) != IFX_OK ||
+        ensure(ctx, ctx->srgb_t, 256 * sizeof(float)) != IFX_OK || ensure(ctx, ctx->ctl, sizeof(SolveCtl)) != IFX_OK)
+        return bail(cudaErrorMemoryAllocation);
+    if ((e = cudaMemsetAsync(ctx->status.p, 0, 16, ctx->st)) != cudaSuccess) return bail(e);
+    float t[256];
+    srgb_thresholds(t);
+    if ((e = cudaMemcpyAsync(ctx->srgb_t.p, t, sizeof t, cudaMemcpyHostToDevice, ctx->st)) != cudaSuccess)
+        return bail(e);
+    configure_kernels((int)kMaxStagedBlob);
+    if ((e = cudaStreamSynchronize(ctx->st)) != cudaSuccess) return bail(e);
+    *out = ctx;
+    return IFX_OK;
+}
+
+extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    DBuf* bufs[] = {&ctx->blob, &ctx->status, &ctx->srgb_t, &ctx->sp, &ctx->sn, &ctx->salb, &ctx->sdir, &ctx->sirr,
+                    &ctx->srad, &ctx->keys, &ctx->keys_alt, &ctx->heads, &ctx->head_scan, &ctx->seg_start,
+                    &ctx->members, &ctx->cp_tmp, &ctx->cn_tmp, &ctx->valid, &ctx->valid_scan, &ctx->cp, &ctx->cn,
+                    &ctx->crange, &ctx->cand_count, &ctx->cand_off, &ctx->cand_c, &ctx->cand_ff, &ctx->cand_row,
+                    &ctx->cand_vis, &ctx->cand_steps, &ctx->row_open, &ctx->row_csteps, &ctx->row_links,
+                    &ctx->row_scale, &ctx->row_sum, &ctx->row_sky, &ctx->row_evals, &ctx->starts, &ctx->idx,
+                    &ctx->w, &ctx->cluster_rad, &ctx->ctl, &ctx->gkeys, &ctx->gkeys_alt, &ctx->gstarts, &ctx->gp,
+                    &ctx->gn, &ctx->girr, &ctx->gitems, &ctx->film, &ctx->out8, &ctx->cub_tmp, &ctx->small,
+                    &ctx->gen_cand};
+    for (DBuf* b : bufs) free_buf(*b);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+}
+
+extern "C" const char* ifx_last_error(const ifx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+extern "C" int ifx_get_stats(const ifx_ctx* ctx, ifx_stats* out) {
+    if (!ctx || !out) return IFX_ERR_INVALID;
+    *out = ctx->stats;
+    out->kernel_launches = ctx->launches;
+    return IFX_OK;
+}
+
+extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
+    if (!ctx || !scene) return fail(ctx, IFX_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    const HScene& s = scene->s;
+    // The device traversal stack holds 64 entries, as the reference's does;
+    // reject a tree that could overflow it (never reached by SAH trees of
+    // scenes within the parser's limits).
+    {
+        std::vector<int> depth(s.nodes.size(), 0);
+        int maxd = 0;
+        for (size_t i = 0; i < s.nodes.size(); ++i) {
+            maxd = std::max(maxd, depth[i]);
+            if (s.nodes[i].count == 0) {
+                depth[i + 1] = depth[i] + 1;
+                depth[(size_t)s.nodes[i].link] = depth[i] + 1;
+            }
+        }
+        if (maxd + 2 > 64) return fail(ctx, IFX_ERR_LIMIT, "BVH deeper than the 64-entry traversal stack");
+    }
+    std::vector<uint8_t> blob = flatten_scene(s);
+    ENSURE(ctx->blob, blob.size());
+    CK(cudaMemcpyAsync(ctx->blob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->scene = s;
+    ctx->blobref.ptr = (const uint8_t*)ctx->blob.p;
+    ctx->blobref.bytes = (uint32_t)blob.size();
+    ctx->blobref.staged = blob.size() <= kMaxStagedBlob ? 1 : 0;
+    ctx->sc = scene_consts(s);
+    ctx->has_scene = true;
+    ctx->has_transfer = false;
+    ctx->has_grid = false;
+    return IFX_OK;
+}
+
+// ------------------------------------------------------------- surfels ---
+extern "C" int ifx_surfels_upload(ifx_ctx* ctx, uint64_t n, const float* p, const float* nrm, const float* albedo,
+                                  const float* area) {
+    if (!ctx || (n && (!p || !nrm || !albedo || !area))) return fail(ctx, IFX_ERR_INVALID, "null argument");
+    if (n > 2000000ull) return fail(ctx, IFX_ERR_LIMIT, "more than 2000000 surfels");
+    CK(cudaSetDevice(ctx->device));
+    std::vector<float4> hp(n), hn(n), ha(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        hp[i] = make_float4(p[3 * i], p[3 * i + 1], p[3 * i + 2], area[i]);
+        hn[i] = make_float4(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2], 0.0f);
+        ha[i] = make_float4(albedo[3 * i], albedo[3 * i + 1], albedo[3 * i + 2], 0.0f);
+    }
+    size_t b = n * sizeof(float4);
+    ENSURE(ctx->sp, b);
+    ENSURE(ctx->sn, b);
+    ENSURE(ctx->salb, b);
+    ENSURE(ctx->sdir, b);
+    ENSURE(ctx->sirr, b);
+    ENSURE(ctx->srad, b);
+    if (n) {
+        CK(cudaMemcpyAsync(ctx->sp.p, hp.data(), b, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->sn.p, hn.data(), b, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->salb.p, ha.data(), b, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemsetAsync(ctx->sdir.p, 0, b, ctx->st));
+        CK(cudaMemsetAsync(ctx->sirr.p, 0, b, ctx->st));
+        CK(cudaMemsetAsync(ctx->srad.p, 0, b, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->n = (uint32_t)n;
+    ctx->has_transfer = false;
+    ctx->has_grid = false;
+    return IFX_OK;
+}
+
+extern "C" int ifx_surfels_count(const ifx_ctx* ctx, uint64_t* n) {
+    if (!ctx || !n) return IFX_ERR_INVALID;
+    *n = ctx->n;
+    return IFX_OK;
+}
+
+static int download3(ifx_ctx* ctx, const DBuf& src, float* dst, bool w_only = false) {
+    if (!dst || ctx->n == 0) return IFX_OK;
+    std::vector<float4> h(ctx->n);
+    CK(cudaMemcpyAsync(h.data(), src.p, ctx->n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (uint32_t i = 0; i < ctx->n; ++i) {
+        if (w_only) {
+            dst[i] = h[i].w;
+        } else {
+            dst[3 * i] = h[i].x;
+            dst[3 * i + 1] = h[i].y;
+            dst[3 * i + 2] = h[i].z;
+        }
+    }
+    return IFX_OK;
+}
+
+extern "C" int ifx_surfels_download(ifx_ctx* ctx, float* p, float* nrm, float* albedo, float* area, float* direct,
+                                    float* irr, float* rad) {
+    if (!ctx) return IFX_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    int r;
+    if ((r = download3(ctx, ctx->sp, p)) || (r = download3(ctx, ctx->sn, nrm)) ||
+        (r = download3(ctx, ctx->salb, albedo)) || (r = download3(ctx, ctx->sp, area, true)) ||
+        (r = download3(ctx, ctx->sdir, direct)) || (r = download3(ctx, ctx->sirr, irr)) ||
+        (r = download3(ctx, ctx->srad, rad)))
+        return r;
+    return IFX_OK;
+}
+
+// surfel.rs:147-255. The projection of every Halton seed runs on the GPU in
+// chunks; the Poisson-disc test is inherently sequential in seed order (a
+// seed is rejected by any earlier accepted surfel within d_min) and runs on
+// the host over the projected points, chunk by chunk, until `target`
+// surfels are placed.
+extern "C" int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* placed) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (target == 0 || target > 2000000ull) return fail(ctx, IFX_ERR_LIMIT, "surfel target out of range");
+    CK(cudaSetDevice(ctx->device));
+    const float* lo = ctx->sc.lo;
+    const float* hi = ctx->sc.hi;
+    const float diag = ctx->sc.diag;
+    const float d_min = std::fmax(diag / std::sqrt((float)target), 1e-4f);
+    const float inv_cell = 1.0f / d_min;
+    const float eps = d_min * 0.02f;
+    const float d_min_sq = d_min * d_min;
+    auto dim_of = [&](int a) {
+        float e = std::ceil((hi[a] - lo[a]) * inv_cell);
+        int v = std::isnan(e) ? 0 : (e >= 2147483648.0f ? 2147483647 : (int)e);
+        return v < 1 ? 1 : (v > 512 ? 512 : v);
+    };
+    const int dim[3] = {dim_of(0), dim_of(1), dim_of(2)};
+    auto cell_of = [&](float v, int a) {
+        float f = (v - lo[a]) * inv_cell;
+        int c = std::isnan(f) ? 0 : (f >= 2147483648.0f ? 2147483647 : (f <= -2147483648.0f ? -2147483647 - 1 : (int)f));
+        return c < 0 ? 0 : (c > dim[a] - 1 ? dim[a] - 1 : c);
+    };
+    uint64_t seeds64 = (uint64_t)(uint32_t)target * 24ull;
+    if (seeds64 > 0xffffffffull) seeds64 = 0xffffffffull;
+    const uint32_t seeds = (uint32_t)(seeds64 < 6000000ull ? seeds64 : 6000000ull);
+
+    // Occupancy: cell -> list of accepted surfels (a hash map, since the
+    // reference's dense cell table reaches 512^3 entries).
+    std::unordered_map<uint64_t, std::vector<uint32_t>> occ;
+    std::vector<float4> acc;
+    acc.reserve((size_t)target);
+    const uint32_t kChunk = 1u << 18;
+    ENSURE(ctx->gen_cand, (size_t)kChunk * sizeof(float4));
+    ctx->gen_host.resize(kChunk);
+    for (uint32_t s0 = 0; s0 < seeds && acc.size() < target; s0 += kChunk) {
+        uint32_t cnt = seeds - s0 < kChunk ? seeds - s0 : kChunk;
+        launch_gen_project(ctx->st, ctx->blobref, ctx->sc, s0, cnt, eps, (float4*)ctx->gen_cand.p,
+                           (uint32_t*)ctx->status.p);
+        ctx->launches++;
+        CKL();
+        CK(cudaMemcpyAsync(ctx->gen_host.data(), ctx->gen_cand.p, cnt * sizeof(float4), cudaMemcpyDeviceToHost,
+                           ctx->st));
+        int r = check_status(ctx);
+        if (r) return r;
+        for (uint32_t j = 0; j < cnt && acc.size() < target; ++j) {
+            const float4 q = ctx->gen_host[j];
+            if (q.w == 0.0f) continue;
+            int c[3] = {cell_of(q.x, 0), cell_of(q.y, 1), cell_of(q.z, 2)};
+            bool close = false;
+            for (int z = std::max(c[2] - 1, 0); z <= std::min(c[2] + 1, dim[2] - 1) && !close; ++z)
+                for (int y = std::max(c[1] - 1, 0); y <= std::min(c[1] + 1, dim[1] - 1) && !close; ++y)
+                    for (int x = std::max(c[0] - 1, 0); x <= std::min(c[0] + 1, dim[0] - 1) && !close; ++x) {
+                        uint64_t key = (uint64_t)x + (uint64_t)dim[0] * ((uint64_t)y + (uint64_t)dim[1] * (uint64_t)z);
+                        auto it = occ.find(key);
+                        if (it == occ.end()) continue;
+                        for (uint32_t k : it->second) {
+                            float dx = acc[k].x - q.x, dy = acc[k].y - q.y, dz = acc[k].z - q.z;
+                            if (dx * dx + dy * dy + dz * dz < d_min_sq) {
+                                close = true;
+                                break;
+                            }
+                        }
+                    }
+            if (close) continue;
+            uint64_t key = (uint64_t)c[0] + (uint64_t)dim[0] * ((uint64_t)c[1] + (uint64_t)dim[1] * (uint64_t)c[2]);
+            occ[key].push_back((uint32_t)acc.size());
+            acc.push_back(q);
+        }
+    }
+    const uint32_t n = (uint32_t)acc.size();
+    size_t b = (size_t)n * sizeof(float4);
+    ENSURE(ctx->sp, b);
+    ENSURE(ctx->sn, b);
+    ENSURE(ctx->salb, b);
+    ENSURE(ctx->sdir, b);
+    ENSURE(ctx->sirr, b);
+    ENSURE(ctx->srad, b);
+    ENSURE(ctx->gen_cand, b);
+    if (n) {
+        CK(cudaMemcpyAsync(ctx->gen_cand.p, acc.data(), b, cudaMemcpyHostToDevice, ctx->st));
+        launch_gen_finalize(ctx->st, ctx->blobref, (const float4*)ctx->gen_cand.p, n, d_min * d_min / 0.65f,
+                            ctx->sarr(), (uint32_t*)ctx->status.p);
+        ctx->launches++;
+        CKL();
+    }
+    int r = check_status(ctx);
+    if (r) return r;
+    ctx->n = n;
+    ctx->has_transfer = false;
+    ctx->has_grid = false;
+    if (placed) *placed = n;
+    return IFX_OK;
+}
+
+// ------------------------------------------------------------ transfer ---
+static int build_clusters(ifx_ctx* ctx, int res) {
+    const uint32_t n = ctx->n;
+    ENSURE(ctx->keys, (size_t)n * 8);
+    ENSURE(ctx->keys_alt, (size_t)n * 8);
+    ENSURE(ctx->heads, (size_t)n * 4);
+    ENSURE(ctx->head_scan, (size_t)n * 4);
+    ENSURE(ctx->members, (size_t)n * 4);
+    ENSURE(ctx->seg_start, ((size_t)n + 1) * 4);
+    ENSURE(ctx->cp_tmp, (size_t)n * 16);
+    ENSURE(ctx->cn_tmp, (size_t)n * 16);
+    ENSURE(ctx->valid, ((size_t)n + 1) * 4);
+    ENSURE(ctx->valid_scan, ((size_t)n + 1) * 4);
+    launch_cluster_keys(ctx->st, (const float4*)ctx->sp.p, (const float4*)ctx->sn.p, n, ctx->sc, res,
+                        (unsigned long long*)ctx->keys.p);
+    ctx->launches++;
+    CKL();
+    unsigned long long maxkey = (unsigned long long)res * res * res * 6ull;
+    int end_bit = 32;
+    while (end_bit < 64 && (1ull << (end_bit - 32)) < maxkey) ++end_bit;
+    auto* kin = (unsigned long long*)ctx->keys.p;
+    auto* kout = (unsigned long long*)ctx->keys_alt.p;
+    CUB([&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortKeys(t, b, kin, kout, (int)n, 0, end_bit, ctx->st);
+    });
+    launch_seg_heads(ctx->st, kout, n, (uint32_t*)ctx->heads.p);
+    ctx->launches++;
+    CKL();
+    CUB([&](void* t, size_t& b) {
+        return cub::DeviceScan::InclusiveSum(t, b, (uint32_t*)ctx->heads.p, (uint32_t*)ctx->head_scan.p, (int)n,
+                                             ctx->st);
+    });
+    launch_seg_starts(ctx->st, kout, (const uint32_t*)ctx->head_scan.p, n, (uint32_t*)ctx->seg_start.p,
+                      (uint32_t*)ctx->members.p);
+    ctx->launches++;
+    CKL();
+    uint32_t nseg = 0;
+    CK(cudaMemcpyAsync(&nseg, (uint32_t*)ctx->head_scan.p + (n - 1), 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    launch_cluster_reduce(ctx->st, (const uint32_t*)ctx->seg_start.p, (const uint32_t*)ctx->members.p, nseg,
+                          (const float4*)ctx->sp.p, (const float4*)ctx->sn.p, (float4*)ctx->cp_tmp.p,
+                          (float4*)ctx->cn_tmp.p, (uint32_t*)ctx->valid.p);
+    ctx->launches++;
+    CKL();
+    CK(cudaMemsetAsync((uint32_t*)ctx->valid.p + nseg, 0, 4, ctx->st));
+    CUB([&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, (uint32_t*)ctx->valid.p, (uint32_t*)ctx->valid_scan.p,
+                                             (int)nseg + 1, ctx->st);
+    });
+    uint32_t nc = 0;
+    CK(cudaMemcpyAsync(&nc, (uint32_t*)ctx->valid_scan.p + nseg, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ENSURE(ctx->cp, (size_t)nc * 16);
+    ENSURE(ctx->cn, (size_t)nc * 16);
+    ENSURE(ctx->crange, (size_t)nc * 8);
+    launch_cluster_compact(ctx->st, (const uint32_t*)ctx->valid.p, (const uint32_t*)ctx->valid_scan.p, nseg,
+                           (const uint32_t*)ctx->seg_start.p, (const float4*)ctx->cp_tmp.p,
+                           (const float4*)ctx->cn_tmp.p, (float4*)ctx->cp.p, (float4*)ctx->cn.p,
+                           (uint2*)ctx->crange.p);
+    ctx->launches++;
+    CKL();
+    ctx->nseg = nseg;
+    ctx->nc = nc;
+    return IFX_OK;
+}
+
+extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (cluster_res < 1 || cluster_res > 512) return fail(ctx, IFX_ERR_LIMIT, "cluster resolution must be in 1..512");
+    if (ctx->n == 0) return fail(ctx, IFX_ERR_INVALID, "no surfels");
+    CK(cudaSetDevice(ctx->device));
+    const uint32_t n = ctx->n;
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    int r = build_clusters(ctx, cluster_res);
+    if (r) return r;
+    const uint32_t nc = ctx->nc;
+    const float4* sp = (const float4*)ctx->sp.p;
+    const float4* sn = (const float4*)ctx->sn.p;
+    const float4* cp = (const float4*)ctx->cp.p;
+    const float4* cn = (const float4*)ctx->cn.p;
+    uint32_t* status = (uint32_t*)ctx->status.p;
+
+    // Candidate pairs.
+    ENSURE(ctx->cand_count, ((size_t)n + 1) * 8);
+    ENSURE(ctx->cand_off, ((size_t)n + 1) * 8);
+    launch_pair_count(ctx->st, sp, sn, n, cp, cn, nc, (unsigned long long*)ctx->cand_count.p);
+    ctx->launches++;
+    CKL();
+    CK(cudaMemsetAsync((unsigned long long*)ctx->cand_count.p + n, 0, 8, ctx->st));
+    CUB([&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, (unsigned long long*)ctx->cand_count.p,
+                                             (unsigned long long*)ctx->cand_off.p, (int)n + 1, ctx->st);
+    });
+    unsigned long long ncand = 0;
+    CK(cudaMemcpyAsync(&ncand, (unsigned long long*)ctx->cand_off.p + n, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ENSURE(ctx->cand_c, ncand * 4);
+    ENSURE(ctx->cand_ff, ncand * 4);
+    ENSURE(ctx->cand_row, ncand * 4);
+    ENSURE(ctx->cand_vis, ncand * 4);
+    ENSURE(ctx->cand_steps, ncand);
+    launch_pair_fill(ctx->st, sp, sn, n, cp, cn, nc, (const unsigned long long*)ctx->cand_off.p,
+                     (uint32_t*)ctx->cand_c.p, (float*)ctx->cand_ff.p, (uint32_t*)ctx->cand_row.p);
+    ctx->launches++;
+    CKL();
+
+    // Visibility and closure.
+    launch_visibility(ctx->st, ctx->blobref, ctx->sc, sp, sn, cp, cn, (const uint32_t*)ctx->cand_c.p,
+                      (const uint32_t*)ctx->cand_row.p, ncand, (float*)ctx->cand_vis.p,
+                      (uint8_t*)ctx->cand_steps.p, status);
+    if (ncand) ctx->launches++;
+    CKL();
+    ENSURE(ctx->row_open, (size_t)n * 4);
+    ENSURE(ctx->row_csteps, (size_t)n * 4);
+    launch_closure(ctx->st, ctx->blobref, ctx->sc, sp, sn, n, (uint32_t*)ctx->row_open.p,
+                   (uint32_t*)ctx->row_csteps.p, status);
+    ctx->launches++;
+    CKL();
+
+    // Rows: links, ordered sums, calibration, CSR.
+    ENSURE(ctx->row_links, ((size_t)n + 1) * 4);
+    ENSURE(ctx->row_scale, (size_t)n * 4);
+    ENSURE(ctx->row_sum, (size_t)n * 4);
+    ENSURE(ctx->row_sky, (size_t)n * 4);
+    ENSURE(ctx->row_evals, (size_t)n * 8);
+    ENSURE(ctx->starts, ((size_t)n + 1) * 4);
+    launch_row_finalize(ctx->st, n, (const unsigned long long*)ctx->cand_off.p, (const float*)ctx->cand_ff.p,
+                        (const float*)ctx->cand_vis.p, (const uint8_t*)ctx->cand_steps.p,
+                        (const uint32_t*)ctx->row_open.p, (const uint32_t*)ctx->row_csteps.p,
+                        (uint32_t*)ctx->row_links.p, (float*)ctx->row_scale.p, (float*)ctx->row_sum.p,
+                        (float*)ctx->row_sky.p, (unsigned long long*)ctx->row_evals.p);
+    ctx->launches++;
+    CKL();
+    CK(cudaMemsetAsync((uint32_t*)ctx->row_links.p + n, 0, 4, ctx->st));
+    CUB([&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, (uint32_t*)ctx->row_links.p, (uint32_t*)ctx->starts.p, (int)n + 1,
+                                             ctx->st);
+    });
+    uint32_t links = 0;
+    CK(cudaMemcpyAsync(&links, (uint32_t*)ctx->starts.p + n, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ENSURE(ctx->idx, (size_t)links * 4);
+    ENSURE(ctx->w, (size_t)links * 4);
+    launch_row_fill(ctx->st, n, (const unsigned long long*)ctx->cand_off.p, (const uint32_t*)ctx->cand_c.p,
+                    (const float*)ctx->cand_ff.p, (const float*)ctx->cand_vis.p, (const float*)ctx->row_scale.p,
+                    (const uint32_t*)ctx->starts.p, (uint32_t*)ctx->idx.p, (float*)ctx->w.p);
+    ctx->launches++;
+    CKL();
+    // small: [0] mean (f32 bits), [1] interior, [2] evals
+    unsigned long long* small = (unsigned long long*)ctx->small.p;
+    CK(cudaMemsetAsync(small, 0, 64, ctx->st));
+    launch_mean_row_sum(ctx->st, n, (const uint32_t*)ctx->starts.p, (const float*)ctx->row_sum.p, (float*)&small[0],
+                        &small[1]);
+    launch_sum_u64(ctx->st, (const unsigned long long*)ctx->row_evals.p, n, &small[2]);
+    ctx->launches += 2;
+    CKL();
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    unsigned long long hs[3];
+    CK(cudaMemcpyAsync(hs, small, 24, cudaMemcpyDeviceToHost, ctx->st));
+    r = check_status(ctx);
+    if (r) return r;
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->stats.ms_transfer = ms;
+    ctx->ncand = ncand;
+    ctx->links = links;
+    ctx->has_transfer = true;
+    ctx->has_grid = false;
+    if (out) {
+        float mean;
+        memcpy(&mean, &hs[0], 4);
+        out->clusters = nc;
+        out->links = links;
+        out->candidates = ncand;
+        out->evals = hs[2];
+        out->interior_rows = hs[1];
+        out->mean_row_sum = mean;
+    }
+    return IFX_OK;
+}
+
+extern "C" int ifx_transfer_download(ifx_ctx* ctx, uint32_t* starts, uint32_t* idx, float* w) {
+    if (!ctx || !ctx->has_transfer) return fail(ctx, IFX_ERR_INVALID, "no transfer");
+    CK(cudaSetDevice(ctx->device));
+    if (starts) CK(cudaMemcpyAsync(starts, ctx->starts.p, ((size_t)ctx->n + 1) * 4, cudaMemcpyDeviceToHost, ctx->st));
+    if (idx && ctx->links) CK(cudaMemcpyAsync(idx, ctx->idx.p, ctx->links * 4, cudaMemcpyDeviceToHost, ctx->st));
+    if (w && ctx->links) CK(cudaMemcpyAsync(w, ctx->w.p, ctx->links * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return IFX_OK;
+}
+
+extern "C" int ifx_clusters_download(ifx_ctx* ctx, float* pnar8, uint32_t* offsets, uint32_t* members) {
+    if (!ctx || ctx->nc == 0) return fail(ctx, IFX_ERR_INVALID, "no clusters");
+    CK(cudaSetDevice(ctx->device));
+    std::vector<float4> cp(ctx->nc), cn(ctx->nc);
+    std::vector<uint2> cr(ctx->nc);
+    std::vector<uint32_t> mem(ctx->n);
+    CK(cudaMemcpyAsync(cp.data(), ctx->cp.p, ctx->nc * 16, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(cn.data(), ctx->cn.p, ctx->nc * 16, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(cr.data(), ctx->crange.p, ctx->nc * 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(mem.data(), ctx->members.p, (size_t)ctx->n * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    uint32_t off = 0;
+    for (uint32_t c = 0; c < ctx->nc; ++c) {
+        if (pnar8) {
+            float* d = pnar8 + 8 * (size_t)c;
+            d[0] = cp[c].x; d[1] = cp[c].y; d[2] = cp[c].z;
+            d[3] = cn[c].x; d[4] = cn[c].y; d[5] = cn[c].z;
+            d[6] = cp[c].w; d[7] = cn[c].w;
+        }
+        if (offsets) offsets[c] = off;
+        for (uint32_t k = cr[c].x; k < cr[c].y; ++k) {
+            if (members) members[off] = mem[k];
+            ++off;
+        }
+    }
+    if (offsets) offsets[ctx->nc] = off;
+    return IFX_OK;
+}
+
+extern "C" int ifx_transfer_row_diag(ifx_ctx* ctx, float* row_sum, float* row_sky, uint64_t* row_evals,
+                                     uint32_t* cand_count) {
+    if (!ctx || !ctx->has_transfer) return fail(ctx, IFX_ERR_INVALID, "no transfer");
+    CK(cudaSetDevice(ctx->device));
+    size_t n = ctx->n;
+    if (row_sum) CK(cudaMemcpyAsync(row_sum, ctx->row_sum.p, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+    if (row_sky) CK(cudaMemcpyAsync(row_sky, ctx->row_sky.p, n * 4, cudaMemcpyDeviceToHost, ctx->st));
+    if (row_evals) CK(cudaMemcpyAsync(row_evals, ctx->row_evals.p, n * 8, cudaMemcpyDeviceToHost, ctx->st));
+    std::vector<unsigned long long> cc;
+    if (cand_count) {
+        cc.resize(n);
+        CK(cudaMemcpyAsync(cc.data(), ctx->cand_count.p, n * 8, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    for (size_t i = 0; i < cc.size(); ++i) cand_count[i] = (uint32_t)cc[i];
+    return IFX_OK;
+}
+
+extern "C" int ifx_transfer_upload(ifx_ctx* ctx, const uint32_t* starts, uint64_t links, const uint32_t* idx,
+                                   const float* w) {
+    if (!ctx || !starts || (links && (!idx || !w))) return fail(ctx, IFX_ERR_INVALID, "null argument");
+    if (ctx->nc == 0) return fail(ctx, IFX_ERR_INVALID, "no clusters: build a transfer first");
+    if (starts[ctx->n] != links) return fail(ctx, IFX_ERR_INVALID, "starts[n] != links");
+    for (uint64_t k = 0; k < links; ++k)
+        if (idx[k] >= ctx->nc) return fail(ctx, IFX_ERR_INVALID, "cluster index out of range");
+    CK(cudaSetDevice(ctx->device));
+    ENSURE(ctx->starts, ((size_t)ctx->n + 1) * 4);
+    ENSURE(ctx->idx, links * 4);
+    ENSURE(ctx->w, links * 4);
+    CK(cudaMemcpyAsync(ctx->starts.p, starts, ((size_t)ctx->n + 1) * 4, cudaMemcpyHostToDevice, ctx->st));
+    if (links) {
+        CK(cudaMemcpyAsync(ctx->idx.p, idx, links * 4, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->w.p, w, links * 4, cudaMemcpyHostToDevice, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->links = links;
+    ctx->has_transfer = true;
+    return IFX_OK;
+}
+
+// --------------------------------------------------------------- solve ---
+extern "C" int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    CK(cudaSetDevice(ctx->device));
+    unsigned long long* small = (unsigned long long*)ctx->small.p;
+    CK(cudaMemsetAsync(small, 0, 8, ctx->st));
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    if (ctx->n) {
+        launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), ctx->n, small, (uint32_t*)ctx->status.p);
+        ctx->launches++;
+        CKL();
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    unsigned long long e = 0;
+    CK(cudaMemcpyAsync(&e, small, 8, cudaMemcpyDeviceToHost, ctx->st));
+    int r = check_status(ctx);
+    if (r) return r;
+    CK(cudaEventElapsedTime(&ctx->stats.ms_light, ctx->ev0, ctx->ev1));
+    ctx->has_grid = false;
+    if (evals) *evals = e;
+    return IFX_OK;
+}
+
+extern "C" int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* out) {
+    if (!ctx || !ctx->has_transfer) return fail(ctx, IFX_ERR_INVALID, "no transfer");
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->nc == 0) {  // solve.rs:49-55
+        if (out) *out = ifx_solve_stats{0, 0.0f};
+        return IFX_OK;
+    }
+    ENSURE(ctx->cluster_rad, (size_t)ctx->nc * 16);
+    SolveCtl* ctl = (SolveCtl*)ctx->ctl.p;
+    CK(cudaMemsetAsync(ctl, 0, sizeof(SolveCtl), ctx->st));
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    SolveCtl h{};
+    // Bounces are enqueued in batches; the host looks at the device-side
+    // convergence flag only between batches.
+    const uint32_t kBatch = 16;
+    for (uint32_t it = 0; it < max_bounces;) {
+        uint32_t end = it + kBatch < max_bounces ? it + kBatch : max_bounces;
+        for (; it < end; ++it) {
+            int l = 0;
+            launch_solve_bounce(ctx->st, ctx->sarr(), ctx->n, (const float4*)ctx->cp.p, (const uint2*)ctx->crange.p,
+                                (const uint32_t*)ctx->members.p, ctx->nc, (const uint32_t*)ctx->starts.p,
+                                (const uint32_t*)ctx->idx.p, (const float*)ctx->w.p, (float4*)ctx->cluster_rad.p,
+                                ctl, it, &l);
+            ctx->launches += (uint64_t)l;
+        }
+        CKL();
+        CK(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (h.done) break;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ctx->stats.ms_solve, ctx->ev0, ctx->ev1));
+    ctx->has_grid = false;
+    if (out) {
+        out->iterations = h.iterations;
+        float res;
+        memcpy(&res, &h.last_residual, 4);
+        out->residual = res;
+    }
+    return IFX_OK;
+}
+
+// --------------------------------------------------------------- shade ---
+extern "C" int ifx_grid_build(ifx_ctx* ctx, float radius) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    CK(cudaSetDevice(ctx->device));
+    const HScene& s = ctx->scene;
+    if (!(radius > 0.0f)) radius = (ctx->sc.diag / std::sqrt((float)s.cfg.surfels)) * 2.6f;  // main.rs:473
+    GridParams g{};
+    // surfel.rs:72-79
+    g.inv_cell = 1.0f / radius;
+    for (int a = 0; a < 3; ++a) {
+        float e = std::ceil((ctx->sc.hi[a] - ctx->sc.lo[a]) * g.inv_cell);
+        int v = std::isnan(e) ? 0 : (e >= 2147483648.0f ? 2147483647 : (int)e);
+        g.dim[a] = v < 1 ? 1 : (v > 512 ? 512 : v);
+        g.lo[a] = ctx->sc.lo[a];
+    }
+    g.radius = radius;
+    const uint32_t n = ctx->n;
+    const uint32_t ncells = (uint32_t)g.dim[0] * (uint32_t)g.dim[1] * (uint32_t)g.dim[2];
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    ENSURE(ctx->gkeys, (size_t)n * 8);
+    ENSURE(ctx->gkeys_alt, (size_t)n * 8);
+    ENSURE(ctx->gstarts, ((size_t)ncells + 1) * 4);
+    ENSURE(ctx->gp, (size_t)n * 16);
+    ENSURE(ctx->gn, (size_t)n * 16);
+    ENSURE(ctx->girr, (size_t)n * 16);
+    ENSURE(ctx->gitems, (size_t)n * 4);
+    auto* kin = (unsigned long long*)ctx->gkeys.p;
+    auto* kout = (unsigned long long*)ctx->gkeys_alt.p;
+    if (n) {
+        launch_grid_keys(ctx->st, (const float4*)ctx->sp.p, n, g, kin);
+        ctx->launches++;
+        CKL();
+        int end_bit = 32;
+        while (end_bit < 64 && (1ull << (end_bit - 32)) < (unsigned long long)ncells) ++end_bit;
+        CUB([&](void* t, size_t& b) {
+            return cub::DeviceRadixSort::SortKeys(t, b, kin, kout, (int)n, 0, end_bit, ctx->st);
+        });
+    }
+    launch_grid_starts(ctx->st, kout, n, ncells, (uint32_t*)ctx->gstarts.p);
+    ctx->launches++;
+    CKL();
+    if (n) {
+        launch_grid_scatter(ctx->st, kout, n, ctx->sarr(), (float4*)ctx->gp.p, (float4*)ctx->gn.p,
+                            (float4*)ctx->girr.p, (uint32_t*)ctx->gitems.p);
+        ctx->launches++;
+        CKL();
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ctx->stats.ms_grid, ctx->ev0, ctx->ev1));
+    g.gp = (const float4*)ctx->gp.p;
+    g.gn = (const float4*)ctx->gn.p;
+    g.girr = (const float4*)ctx->girr.p;
+    g.starts = (const uint32_t*)ctx->gstarts.p;
+    ctx->grid = g;
+    ctx->ncells = ncells;
+    ctx->has_grid = true;
+    return IFX_OK;
+}
+
+extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
+                                float* out_linear, uint8_t* out_srgb, uint64_t* evals) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (mode < 0 || mode > 5) return fail(ctx, IFX_ERR_INVALID, "unknown mode");
+    if (w == 0 || h == 0 || w > 16384u || h > 16384u || (uint64_t)w * h > 40000000ull)
+        return fail(ctx, IFX_ERR_LIMIT, "film size out of range");
+    CK(cudaSetDevice(ctx->device));
+    const HScene& s = ctx->scene;
+    F3 pos = s.camera.pos, look = s.camera.look, up = s.camera.up;
+    float fov = s.camera.fov;
+    if (cam) {
+        pos = F3{cam->pos[0], cam->pos[1], cam->pos[2]};
+        look = F3{cam->look[0], cam->look[1], cam->look[2]};
+        up = F3{cam->up[0], cam->up[1], cam->up[2]};
+        fov = cam->fov;
+    }
+    CamBasis b = camera_basis(pos, look, up, fov, w, h);
+    ShadeParams P{};
+    P.blob = ctx->blobref;
+    const bool needs_gi = mode == IFX_MODE_BEAUTY || mode == IFX_MODE_INDIRECT;
+    P.has_gi = needs_gi && ctx->has_grid ? 1 : 0;
+    P.grid = ctx->grid;
+    memcpy(P.cam.origin, b.origin, 12);
+    memcpy(P.cam.fwd, b.fwd, 12);
+    memcpy(P.cam.right, b.right, 12);
+    memcpy(P.cam.up, b.up, 12);
+    P.cam.tan_half = b.tan_half;
+    P.cam.aspect = b.aspect;
+    P.w = w;
+    P.h = h;
+    P.tmax = ctx->sc.diag * 4.0f;  // main.rs:417
+    P.mode = mode;
+    P.exposure = exposure;
+    P.tonemap = mode <= IFX_MODE_INDIRECT ? 1 : 0;
+    P.srgb_t = (const float*)ctx->srgb_t.p;
+    size_t px = (size_t)w * h;
+    if (out_linear) {
+        ENSURE(ctx->film, px * 12);
+        P.film = (float*)ctx->film.p;
+    }
+    if (out_srgb) {
+        ENSURE(ctx->out8, px * 3);
+        P.out8 = (uint8_t*)ctx->out8.p;
+    }
+    unsigned long long* small = (unsigned long long*)ctx->small.p;
+    P.evals = &small[3];
+    P.status = (uint32_t*)ctx->status.p;
+    CK(cudaMemsetAsync(&small[3], 0, 8, ctx->st));
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    launch_shade(ctx->st, P);
+    ctx->launches++;
+    CKL();
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    unsigned long long e = 0;
+    CK(cudaMemcpyAsync(&e, &small[3], 8, cudaMemcpyDeviceToHost, ctx->st));
+    if (out_linear) CK(cudaMemcpyAsync(out_linear, ctx->film.p, px * 12, cudaMemcpyDeviceToHost, ctx->st));
+    if (out_srgb) CK(cudaMemcpyAsync(out_srgb, ctx->out8.p, px * 3, cudaMemcpyDeviceToHost, ctx->st));
+    int r = check_status(ctx);
+    if (r) return r;
+    CK(cudaEventElapsedTime(&ctx->stats.ms_shade, ctx->ev0, ctx->ev1));
+    if (evals) *evals = e;
+    return IFX_OK;
+}

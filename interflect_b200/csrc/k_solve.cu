@@ -1,0 +1,105 @@
+// Direct light on surfels (solve.rs:27-39) and the Jacobi bounce solve
+// (solve.rs:47-108). The bounce loop runs without host round trips: every
+// bounce kernel first reads a device-side `done` flag, so the host enqueues
+// max_bounces bounces at once and the ones after convergence return
+// immediately.
+#include "kcommon.cuh"
+
+namespace ifx {
+
+__device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long* out) {
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(out, v);
+}
+
+// solve.rs:27-39
+__global__ void __launch_bounds__(128) k_light_surfels(BlobRef blob, SurfelArrays s, uint32_t n,
+                                                        unsigned long long* evals, uint32_t* status) {
+    IFX_SCENE_PROLOGUE(blob, status, sv);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t limit = (n + stride - 1) / stride * stride;  // keep whole warps for the reduction
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < limit; i += stride) {
+        unsigned long long e = 0;
+        if (i < n) {
+            uint32_t steps = 0;
+            V c = direct_diffuse(sv, mk4(s.p[i]), mk4(s.n[i]), mk4(s.albedo[i]), steps);
+            s.direct[i] = f4(c, 0.0f);
+            s.rad[i] = f4(c, 0.0f);
+            s.irr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            e = steps;
+        }
+        block_add_u64(e, evals);
+    }
+}
+
+// solve.rs:61-73: cluster radiosity as the area-weighted mean of its
+// members' radiosity, summed sequentially in member order.
+__global__ void __launch_bounds__(128) k_cluster_agg(const float4* rad, const float4* sp, const float4* cp,
+                                                      const uint2* crange, const uint32_t* members, uint32_t nc,
+                                                      float4* cluster_rad, const SolveCtl* ctl) {
+    if (ctl->done) return;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        uint2 r = crange[c];
+        V acc{0.0f, 0.0f, 0.0f};
+        for (uint32_t k = r.x; k < r.y; ++k) {
+            uint32_t m = __ldg(&members[k]);
+            acc = acc + mk4(rad[m]) * __ldg(&sp[m].w);
+        }
+        cluster_rad[c] = f4(acc / fmaxf(cp[c].w, 1e-12f), 0.0f);
+    }
+}
+
+// solve.rs:76-102: one Jacobi row per thread, links summed in CSR order;
+// the bounce residual is the maximum change over rows, an order-free
+// reduction kept as the bits of a non-negative f32 (NaN ignored, as the
+// reference's f32::max fold does).
+__global__ void __launch_bounds__(256) k_jacobi(float4* direct, float4* albedo, float4* irr_out, float4* rad,
+                                                 uint32_t n, const uint32_t* starts, const uint32_t* idx,
+                                                 const float* w, const float4* cluster_rad, SolveCtl* ctl) {
+    if (ctl->done) return;
+    float dmax = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        V irr{0.0f, 0.0f, 0.0f};
+        const uint32_t e = starts[i + 1];
+        for (uint32_t k = starts[i]; k < e; ++k) irr = irr + mk4(__ldg(&cluster_rad[__ldg(&idx[k])])) * __ldg(&w[k]);
+        V nr = mk4(direct[i]) + mk4(albedo[i]) * irr;
+        V diff = vabs(nr - mk4(rad[i]));
+        float d = fmaxf(diff.x, fmaxf(diff.y, diff.z));
+        irr_out[i] = f4(irr, 0.0f);
+        rad[i] = f4(nr, 0.0f);
+        if (!isnan(d)) dmax = fmaxf(dmax, d);
+    }
+    for (int o = 16; o >= 1; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
+    if ((threadIdx.x & 31) == 0 && dmax > 0.0f) atomicMax(&ctl->residual_bits, __float_as_uint(dmax));
+}
+
+// solve.rs:454-462
+__global__ void k_bounce_end(SolveCtl* ctl, uint32_t it) {
+    if (ctl->done) return;
+    float res = __uint_as_float(ctl->residual_bits);
+    ctl->iterations = it + 1;
+    ctl->last_residual = ctl->residual_bits;
+    ctl->residual_bits = 0;
+    if (res < 1e-4f) ctl->done = 1;
+}
+
+void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_t n, unsigned long long* evals,
+                          uint32_t* status) {
+    k_light_surfels<<<grid_for(n, 128, 16), 128, blob_smem(blob), st>>>(blob, s, n, evals, status);
+}
+
+void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
+                         const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
+                         const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches) {
+    k_cluster_agg<<<grid_for(nc, 128), 128, 0, st>>>(s.rad, s.p, cp, crange, members, nc, cluster_rad, ctl);
+    k_jacobi<<<grid_for(n, 256), 256, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, starts, idx, w, cluster_rad,
+                                               ctl);
+    k_bounce_end<<<1, 1, 0, st>>>(ctl, it);
+    *launches += 3;
+}
+
+void configure_solve_kernels(int max_dyn_smem) {
+    cudaFuncSetAttribute(k_light_surfels, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+}
+
+}  // namespace ifx

@@ -1,0 +1,218 @@
+// Surfel generation (projection part), surfel clusters and the gather grid.
+#include "kcommon.cuh"
+
+namespace ifx {
+
+// surfel.rs:366-393: Halton seed i (bases 2, 3, 5) across the scene bounds,
+// Newton projection onto the zero level set (at most 10 steps), then the
+// on-surface and in-bounds tests. Writes the projected point with w = 1 if
+// the seed survives, w = 0 otherwise. The Poisson-disc thinning that follows
+// is sequential in seed order and runs on the host.
+__global__ void __launch_bounds__(128) k_gen_project(BlobRef blob, SceneConsts sc, uint32_t seed0,
+                                                      uint32_t count, float eps, float4* out, uint32_t* status) {
+    IFX_SCENE_PROLOGUE(blob, status, sv);
+    const V lo{sc.lo[0], sc.lo[1], sc.lo[2]}, hi{sc.hi[0], sc.hi[1], sc.hi[2]};
+    const float diag = sc.diag;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+        uint32_t i = seed0 + j;
+        V s{radical_inverse(i + 1, 2), radical_inverse(i + 1, 3), radical_inverse(i + 1, 5)};
+        V p = lo + (hi - lo) * s;
+        bool ok = false;
+        for (int it = 0; it < 10; ++it) {
+            float d = scene_dist(sv, p);
+            if (fabsf(d) < eps) {
+                ok = true;
+                break;
+            }
+            if (!isfinite(d) || fabsf(d) > diag) break;
+            p = p - scene_normal(sv, p) * d;
+        }
+        if (ok && fabsf(scene_dist(sv, p)) >= eps) ok = false;
+        if (ok && (p.x < lo.x || p.y < lo.y || p.z < lo.z || p.x > hi.x || p.y > hi.y || p.z > hi.z)) ok = false;
+        out[j] = make_float4(p.x, p.y, p.z, ok ? 1.0f : 0.0f);
+    }
+}
+
+// surfel.rs:415-432: material albedo and normal of each accepted point.
+__global__ void __launch_bounds__(128) k_gen_finalize(BlobRef blob, const float4* pts, uint32_t n, float area,
+                                                       SurfelArrays s, uint32_t* status) {
+    IFX_SCENE_PROLOGUE(blob, status, sv);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        V p = mk4(pts[i]);
+        DistHit h = dist_mat(sv, p);
+        const DMaterial& m = sv.mats[h.mat];
+        V nn = scene_normal(sv, p);
+        s.p[i] = f4(p, area);
+        s.n[i] = f4(nn, 0.0f);
+        s.albedo[i] = make_float4(m.kd[0], m.kd[1], m.kd[2], 0.0f);
+        s.direct[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        s.irr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        s.rad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+void launch_gen_project(cudaStream_t st, BlobRef blob, SceneConsts sc, uint32_t seed0, uint32_t count, float eps,
+                        float4* out, uint32_t* status) {
+    k_gen_project<<<grid_for(count, 128), 128, blob_smem(blob), st>>>(blob, sc, seed0, count, eps, out, status);
+}
+void launch_gen_finalize(cudaStream_t st, BlobRef blob, const float4* pts, uint32_t n, float area, SurfelArrays s,
+                         uint32_t* status) {
+    k_gen_finalize<<<grid_for(n, 128), 128, blob_smem(blob), st>>>(blob, pts, n, area, s, status);
+}
+
+// ------------------------------------------------------------ clusters ----
+// formfactor.rs:70-89
+__device__ __forceinline__ uint32_t normal_bucket(V n) {
+    V a = vabs(n);
+    if (a.x >= a.y && a.x >= a.z) return n.x >= 0.0f ? 0u : 1u;
+    if (a.y >= a.z) return n.y >= 0.0f ? 2u : 3u;
+    return n.z >= 0.0f ? 4u : 5u;
+}
+
+// formfactor.rs:100-110: key (x, y, z, bucket) packed so that integer order
+// is the tuple order; the surfel index in the low word makes the sort
+// stable (members ascend within a cluster, as the reference's push order).
+__global__ void k_cluster_keys(const float4* p, const float4* n, uint32_t count, SceneConsts sc, int res,
+                               unsigned long long* keys) {
+    const V lo{sc.lo[0], sc.lo[1], sc.lo[2]};
+    V ext = V{sc.hi[0], sc.hi[1], sc.hi[2]} - lo;
+    V inv{(float)res / fmaxf(ext.x, 1e-6f), (float)res / fmaxf(ext.y, 1e-6f), (float)res / fmaxf(ext.z, 1e-6f)};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        V c = (mk4(p[i]) - lo) * inv;
+        unsigned long long x = (unsigned long long)clampi(as_i32(c.x), 0, res - 1);
+        unsigned long long y = (unsigned long long)clampi(as_i32(c.y), 0, res - 1);
+        unsigned long long z = (unsigned long long)clampi(as_i32(c.z), 0, res - 1);
+        unsigned long long key = ((x * (unsigned long long)res + y) * (unsigned long long)res + z) * 6ull +
+                                 normal_bucket(mk4(n[i]));
+        keys[i] = (key << 32) | (unsigned long long)i;
+    }
+}
+
+__global__ void k_seg_heads(const unsigned long long* s, uint32_t count, uint32_t* heads) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
+        heads[j] = (j == 0 || (s[j] >> 32) != (s[j - 1] >> 32)) ? 1u : 0u;
+}
+
+// head_scan is the inclusive scan of heads: the segment of position j is
+// head_scan[j] - 1.
+__global__ void k_seg_starts(const unsigned long long* s, const uint32_t* head_scan, uint32_t count,
+                             uint32_t* seg_start, uint32_t* members) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+        members[j] = (uint32_t)(s[j] & 0xffffffffull);
+        uint32_t seg = head_scan[j] - 1u;
+        if (j == 0 || head_scan[j] != head_scan[j - 1]) seg_start[seg] = j;
+        if (j == count - 1) seg_start[seg + 1] = count;
+    }
+}
+
+// formfactor.rs:119-145: sequential area-weighted sums in member order.
+__global__ void k_cluster_reduce(const uint32_t* seg_start, const uint32_t* members, uint32_t nseg,
+                                 const float4* sp, const float4* sn, float4* cp, float4* cn, uint32_t* valid) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nseg; c += gridDim.x * blockDim.x) {
+        V p{0.0f, 0.0f, 0.0f}, n{0.0f, 0.0f, 0.0f};
+        float area = 0.0f;
+        for (uint32_t k = seg_start[c]; k < seg_start[c + 1]; ++k) {
+            uint32_t m = members[k];
+            float4 a = __ldg(&sp[m]);
+            float4 b = __ldg(&sn[m]);
+            p = p + mk4(a) * a.w;
+            n = n + mk4(b) * a.w;
+            area += a.w;
+        }
+        bool ok = area > 1e-12f;
+        valid[c] = ok ? 1u : 0u;
+        V nn = dot(n, n) > 1e-12f ? nrm(n) : V{0.0f, 1.0f, 0.0f};
+        cp[c] = f4(p / area, area);
+        cn[c] = f4(nn, sqrtf(area / kPiF));
+    }
+}
+
+__global__ void k_cluster_compact(const uint32_t* valid, const uint32_t* valid_scan, uint32_t nseg,
+                                  const uint32_t* seg_start, const float4* cp_in, const float4* cn_in, float4* cp,
+                                  float4* cn, uint2* crange) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nseg; c += gridDim.x * blockDim.x) {
+        if (!valid[c]) continue;
+        uint32_t o = valid_scan[c];  // exclusive scan
+        cp[o] = cp_in[c];
+        cn[o] = cn_in[c];
+        crange[o] = make_uint2(seg_start[c], seg_start[c + 1]);
+    }
+}
+
+void launch_cluster_keys(cudaStream_t st, const float4* p, const float4* n, uint32_t count, SceneConsts sc,
+                         int res, unsigned long long* keys) {
+    k_cluster_keys<<<grid_for(count, 256), 256, 0, st>>>(p, n, count, sc, res, keys);
+}
+void launch_seg_heads(cudaStream_t st, const unsigned long long* sorted, uint32_t count, uint32_t* heads) {
+    k_seg_heads<<<grid_for(count, 256), 256, 0, st>>>(sorted, count, heads);
+}
+void launch_seg_starts(cudaStream_t st, const unsigned long long* sorted, const uint32_t* head_scan,
+                       uint32_t count, uint32_t* seg_start, uint32_t* members) {
+    k_seg_starts<<<grid_for(count, 256), 256, 0, st>>>(sorted, head_scan, count, seg_start, members);
+}
+void launch_cluster_reduce(cudaStream_t st, const uint32_t* seg_start, const uint32_t* members, uint32_t nseg,
+                           const float4* sp, const float4* sn, float4* cp, float4* cn, uint32_t* valid) {
+    k_cluster_reduce<<<grid_for(nseg, 64), 64, 0, st>>>(seg_start, members, nseg, sp, sn, cp, cn, valid);
+}
+void launch_cluster_compact(cudaStream_t st, const uint32_t* valid, const uint32_t* valid_scan, uint32_t nseg,
+                            const uint32_t* seg_start, const float4* cp_in, const float4* cn_in, float4* cp,
+                            float4* cn, uint2* crange) {
+    k_cluster_compact<<<grid_for(nseg, 256), 256, 0, st>>>(valid, valid_scan, nseg, seg_start, cp_in, cn_in, cp, cn,
+                                                           crange);
+}
+
+// ---------------------------------------------------------------- grid ----
+// surfel.rs:262-269 cell index; key = (cell << 32) | surfel so that a sort
+// reproduces the counting sort's stable order.
+__global__ void k_grid_keys(const float4* p, uint32_t n, GridParams g, unsigned long long* keys) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 q = p[i];
+        int cx = clampi(as_i32((q.x - g.lo[0]) * g.inv_cell), 0, g.dim[0] - 1);
+        int cy = clampi(as_i32((q.y - g.lo[1]) * g.inv_cell), 0, g.dim[1] - 1);
+        int cz = clampi(as_i32((q.z - g.lo[2]) * g.inv_cell), 0, g.dim[2] - 1);
+        unsigned long long c =
+            (unsigned long long)cx + (unsigned long long)g.dim[0] * ((unsigned long long)cy +
+                                                                     (unsigned long long)g.dim[1] * (unsigned long long)cz);
+        keys[i] = (c << 32) | (unsigned long long)i;
+    }
+}
+
+// starts[c] = first sorted position whose cell is >= c (CSR offsets of the
+// counting sort, surfel.rs:271-279), for every c in [0, ncells].
+__global__ void k_grid_starts(const unsigned long long* s, uint32_t n, uint32_t ncells, uint32_t* starts) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j <= n; j += gridDim.x * blockDim.x) {
+        unsigned long long lo_c = (j == 0) ? 0ull : (s[j - 1] >> 32) + 1ull;
+        unsigned long long hi_c = (j == n) ? (unsigned long long)ncells : (s[j] >> 32);
+        for (unsigned long long c = lo_c; c <= hi_c; ++c) starts[c] = j;
+    }
+}
+
+__global__ void k_grid_scatter(const unsigned long long* s, uint32_t n, SurfelArrays sa, float4* gp, float4* gn,
+                               float4* girr, uint32_t* items) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        uint32_t i = (uint32_t)(s[j] & 0xffffffffull);
+        items[j] = i;
+        gp[j] = sa.p[i];
+        gn[j] = sa.n[i];
+        girr[j] = sa.irr[i];
+    }
+}
+
+void launch_grid_keys(cudaStream_t st, const float4* p, uint32_t n, GridParams g, unsigned long long* keys) {
+    k_grid_keys<<<grid_for(n, 256), 256, 0, st>>>(p, n, g, keys);
+}
+void launch_grid_starts(cudaStream_t st, const unsigned long long* sorted, uint32_t n, uint32_t ncells,
+                        uint32_t* starts) {
+    k_grid_starts<<<grid_for((unsigned long long)n + 1, 256), 256, 0, st>>>(sorted, n, ncells, starts);
+}
+void launch_grid_scatter(cudaStream_t st, const unsigned long long* sorted, uint32_t n, SurfelArrays s,
+                         float4* gp, float4* gn, float4* girr, uint32_t* items) {
+    k_grid_scatter<<<grid_for(n, 256), 256, 0, st>>>(sorted, n, s, gp, gn, girr, items);
+}
+
+void configure_surfel_kernels(int max_dyn_smem) {
+    cudaFuncSetAttribute(k_gen_project, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_gen_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+}
+
+}  // namespace ifx

@@ -1,0 +1,294 @@
+// Transfer build (formfactor.rs:153-277) as a deterministic pipeline:
+//   pair count -> scan -> pair fill      candidate (row, cluster) pairs in
+//                                        cluster order within each row
+//   visibility                           one cone-traced soft shadow per pair
+//   closure                              16 hemisphere rays per row
+//   row finalize -> scan -> row fill     link test, ordered row sum,
+//                                        calibration, CSR in row order
+// Nothing depends on scheduling: every value lands at an index fixed by the
+// scans, and the only float reductions (row sums) run sequentially in the
+// reference's order.
+#include "kcommon.cuh"
+
+namespace ifx {
+
+// formfactor.rs:169-192: facing test and Nusselt disc form factor with the
+// 2e-5 cull. Returns ff, or -1 when the pair is culled.
+__device__ __forceinline__ float pair_ff(V sp, V sn, float4 cp, float4 cn) {
+    V d = mk4(cp) - sp;
+    float r2 = dot(d, d);
+    if (r2 < 1e-9f) return -1.0f;
+    float r = sqrtf(r2);
+    V dir = d / r;
+    float cos_i = dot(sn, dir);
+    float cos_c = dot(mk4(cn), -dir);
+    if (cos_i <= 1e-3f || cos_c <= 1e-3f) return -1.0f;
+    float ff = cos_i * cos_c * cp.w / (kPiF * r2 + cp.w);
+    if (ff < 2e-5f) return -1.0f;
+    return ff;
+}
+
+// One warp per surfel row; lanes stride over clusters.
+__global__ void __launch_bounds__(256) k_pair_count(const float4* sp, const float4* sn, uint32_t n,
+                                                     const float4* cp, const float4* cn, uint32_t nc,
+                                                     unsigned long long* cand_count) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
+        V p = mk4(sp[row]), nn = mk4(sn[row]);
+        uint32_t cnt = 0;
+        for (uint32_t c0 = 0; c0 < nc; c0 += 32) {
+            uint32_t c = c0 + lane;
+            bool pass = c < nc && pair_ff(p, nn, __ldg(&cp[c]), __ldg(&cn[c])) >= 0.0f;
+            cnt += __popc(__ballot_sync(kFull, pass));
+        }
+        if (lane == 0) cand_count[row] = cnt;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_pair_fill(const float4* sp, const float4* sn, uint32_t n,
+                                                    const float4* cp, const float4* cn, uint32_t nc,
+                                                    const unsigned long long* cand_off, uint32_t* cand_c,
+                                                    float* cand_ff, uint32_t* cand_row) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
+        V p = mk4(sp[row]), nn = mk4(sn[row]);
+        unsigned long long at = cand_off[row];
+        for (uint32_t c0 = 0; c0 < nc; c0 += 32) {
+            uint32_t c = c0 + lane;
+            float ff = c < nc ? pair_ff(p, nn, __ldg(&cp[c]), __ldg(&cn[c])) : -1.0f;
+            unsigned mask = __ballot_sync(kFull, ff >= 0.0f);
+            if (ff >= 0.0f) {
+                unsigned long long j = at + __popc(mask & ((1u << lane) - 1u));
+                cand_c[j] = c;
+                cand_ff[j] = ff;
+                cand_row[j] = row;
+            }
+            at += __popc(mask);
+        }
+    }
+}
+
+// formfactor.rs:194-205: the visibility cone of one candidate pair.
+__global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc, const float4* sp,
+                                                     const float4* sn, const float4* cp, const float4* cn,
+                                                     const uint32_t* cand_c, const uint32_t* cand_row,
+                                                     unsigned long long ncand, float* cand_vis,
+                                                     uint8_t* cand_steps, uint32_t* status) {
+    IFX_SCENE_PROLOGUE(blob, status, sv);
+    const float off = sc.diag * 5e-4f, tmin = sc.diag * 1e-3f;
+    for (unsigned long long j = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j < ncand;
+         j += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint32_t row = cand_row[j], c = cand_c[j];
+        const V p = mk4(__ldg(&sp[row])), nn = mk4(__ldg(&sn[row]));
+        const float4 cpc = __ldg(&cp[c]), cnc = __ldg(&cn[c]);
+        V d = mk4(cpc) - p;
+        float r = sqrtf(dot(d, d));
+        V dir = d / r;
+        float k = clampr(r / fmaxf(cnc.w, 1e-4f), 1.5f, 32.0f);
+        uint32_t steps;
+        float vis = soft_shadow(sv, p + nn * off, dir, tmin, r - cnc.w * 0.75f, k, steps);
+        cand_vis[j] = vis;
+        cand_steps[j] = (uint8_t)steps;
+    }
+}
+
+// trace.rs:165-186: 16 lanes per row (one ray each); lane 0 of the 16
+// writes the row's open-ray count and the rays' SDF evaluations. A hit's
+// normal is never used here, so it is not computed, but its four taps are
+// still counted (trace.rs:48).
+__global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, const float4* sp,
+                                                  const float4* sn, uint32_t n, uint32_t* row_open,
+                                                  uint32_t* row_csteps, uint32_t* status) {
+    IFX_SCENE_PROLOGUE(blob, status, sv);
+    const int lane = threadIdx.x & 31;
+    const unsigned long long total = (unsigned long long)n * 16ull;
+    const unsigned long long padded = (total + 31ull) & ~31ull;
+    const float tmax = sc.diag * 2.0f;
+    for (unsigned long long g = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; g < padded;
+         g += (unsigned long long)gridDim.x * blockDim.x) {
+        const bool valid = g < total;
+        uint32_t open = 0, steps = 0;
+        if (valid) {
+            const uint32_t row = (uint32_t)(g >> 4), k = (uint32_t)(g & 15ull);
+            const V p = mk4(__ldg(&sp[row])), nn = mk4(__ldg(&sn[row]));
+            V t, b;
+            frame(nn, t, b);
+            V d = t * sc.closure[k][0] + b * sc.closure[k][1] + nn * sc.closure[k][2];
+            TraceHit h = trace(sv, p + nn * 1e-3f, nrm(d), 1e-3f, tmax);
+            open = h.hit ? 0u : 1u;
+            steps = h.steps;
+        }
+        unsigned om = __ballot_sync(kFull, open != 0);
+        for (int o = 8; o >= 1; o >>= 1) steps += __shfl_xor_sync(kFull, steps, o);
+        if (valid && (lane & 15) == 0) {
+            const uint32_t row = (uint32_t)(g >> 4);
+            row_open[row] = __popc(om & (0xffffu << (lane & 16)));
+            row_csteps[row] = steps;
+        }
+    }
+}
+
+// formfactor.rs:206-238: links are pairs with vis > 1e-3, weighted ff*vis,
+// summed in cluster order; the row is rescaled to 1 - sky (capped at 8x)
+// when its sum exceeds 1e-5. One warp per row; the ordered sum is carried
+// lane-uniformly through the set bits of each 32-candidate chunk.
+__global__ void __launch_bounds__(256) k_row_finalize(uint32_t n, const unsigned long long* cand_off,
+                                                       const float* cand_ff, const float* cand_vis,
+                                                       const uint8_t* cand_steps, const uint32_t* row_open,
+                                                       const uint32_t* row_csteps, uint32_t* row_links,
+                                                       float* row_scale, float* row_sum, float* row_sky,
+                                                       unsigned long long* row_evals) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
+        const unsigned long long b = cand_off[row], e = cand_off[row + 1];
+        float sum = 0.0f;
+        uint32_t links = 0, steps = 0;
+        for (unsigned long long base = b; base < e; base += 32) {
+            unsigned long long j = base + lane;
+            bool valid = j < e;
+            float vis = valid ? cand_vis[j] : 0.0f;
+            float v = valid ? cand_ff[j] * vis : 0.0f;
+            steps += valid ? cand_steps[j] : 0u;
+            unsigned mask = __ballot_sync(kFull, valid && vis > 1e-3f);
+            links += __popc(mask);
+            while (mask) {
+                int k = __ffs(mask) - 1;
+                sum += __shfl_sync(kFull, v, k);
+                mask &= mask - 1;
+            }
+        }
+        for (int o = 16; o >= 1; o >>= 1) steps += __shfl_xor_sync(kFull, steps, o);
+        if (lane == 0) {
+            float sky = (float)row_open[row] / 16.0f;
+            float target = clampr(1.0f - sky, 0.0f, 1.0f);
+            float scale = 1.0f;
+            if (sum > 1e-5f) {
+                scale = fminf(target / sum, 8.0f);
+                sum *= scale;
+            }
+            row_links[row] = links;
+            row_scale[row] = scale;
+            row_sum[row] = fminf(sum, 1.0f);
+            row_sky[row] = sky;
+            row_evals[row] = (unsigned long long)steps + row_csteps[row];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_row_fill(uint32_t n, const unsigned long long* cand_off,
+                                                   const uint32_t* cand_c, const float* cand_ff,
+                                                   const float* cand_vis, const float* row_scale,
+                                                   const uint32_t* starts, uint32_t* idx, float* w) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
+        const unsigned long long b = cand_off[row], e = cand_off[row + 1];
+        const float scale = row_scale[row];
+        uint32_t at = starts[row];
+        for (unsigned long long base = b; base < e; base += 32) {
+            unsigned long long j = base + lane;
+            bool valid = j < e;
+            float vis = valid ? cand_vis[j] : 0.0f;
+            bool link = valid && vis > 1e-3f;
+            unsigned mask = __ballot_sync(kFull, link);
+            if (link) {
+                uint32_t o = at + __popc(mask & ((1u << lane) - 1u));
+                idx[o] = cand_c[j];
+                w[o] = (cand_ff[j] * vis) * scale;
+            }
+            at += __popc(mask);
+        }
+    }
+}
+
+// formfactor.rs:242-253: sequential f32 sum in row order (the reference's
+// iterator sum starts from -0.0), by one thread.
+__global__ void k_mean_row_sum(uint32_t n, const uint32_t* starts, const float* row_sum, float* out_mean,
+                               unsigned long long* out_interior) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    float acc = -0.0f;
+    unsigned long long interior = 0;
+    uint32_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint32_t s[9];
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) s[k] = starts[i + k];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = row_sum[i + k];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (s[k + 1] > s[k]) {
+                acc += v[k];
+                ++interior;
+            }
+    }
+    for (; i < n; ++i)
+        if (starts[i + 1] > starts[i]) {
+            acc += row_sum[i];
+            ++interior;
+        }
+    *out_mean = interior ? acc / (float)interior : 0.0f;
+    *out_interior = interior;
+}
+
+__global__ void k_sum_u64(const unsigned long long* v, uint32_t n, unsigned long long* out) {
+    unsigned long long s = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += v[i];
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
+}
+
+void launch_pair_count(cudaStream_t st, const float4* sp, const float4* sn, uint32_t n, const float4* cp,
+                       const float4* cn, uint32_t nc, unsigned long long* cand_count) {
+    k_pair_count<<<grid_for((unsigned long long)n * 32ull, 256), 256, 0, st>>>(sp, sn, n, cp, cn, nc, cand_count);
+}
+void launch_pair_fill(cudaStream_t st, const float4* sp, const float4* sn, uint32_t n, const float4* cp,
+                      const float4* cn, uint32_t nc, const unsigned long long* cand_off, uint32_t* cand_c,
+                      float* cand_ff, uint32_t* cand_row) {
+    k_pair_fill<<<grid_for((unsigned long long)n * 32ull, 256), 256, 0, st>>>(sp, sn, n, cp, cn, nc, cand_off,
+                                                                             cand_c, cand_ff, cand_row);
+}
+void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
+                       const float4* cp, const float4* cn, const uint32_t* cand_c, const uint32_t* cand_row,
+                       unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status) {
+    if (ncand == 0) return;
+    k_visibility<<<grid_for(ncand, 128, 16), 128, blob_smem(blob), st>>>(blob, sc, sp, sn, cp, cn, cand_c, cand_row,
+                                                                        ncand, cand_vis, cand_steps, status);
+}
+void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
+                    uint32_t n, uint32_t* row_open, uint32_t* row_csteps, uint32_t* status) {
+    k_closure<<<grid_for((unsigned long long)n * 16ull, 128, 16), 128, blob_smem(blob), st>>>(
+        blob, sc, sp, sn, n, row_open, row_csteps, status);
+}
+void launch_row_finalize(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const float* cand_ff,
+                         const float* cand_vis, const uint8_t* cand_steps, const uint32_t* row_open,
+                         const uint32_t* row_csteps, uint32_t* row_links, float* row_scale, float* row_sum,
+                         float* row_sky, unsigned long long* row_evals) {
+    k_row_finalize<<<grid_for((unsigned long long)n * 32ull, 256), 256, 0, st>>>(
+        n, cand_off, cand_ff, cand_vis, cand_steps, row_open, row_csteps, row_links, row_scale, row_sum, row_sky,
+        row_evals);
+}
+void launch_row_fill(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const uint32_t* cand_c,
+                     const float* cand_ff, const float* cand_vis, const float* row_scale, const uint32_t* starts,
+                     uint32_t* idx, float* w) {
+    k_row_fill<<<grid_for((unsigned long long)n * 32ull, 256), 256, 0, st>>>(n, cand_off, cand_c, cand_ff, cand_vis,
+                                                                            row_scale, starts, idx, w);
+}
+void launch_mean_row_sum(cudaStream_t st, uint32_t n, const uint32_t* starts, const float* row_sum,
+                         float* out_mean, unsigned long long* out_interior) {
+    k_mean_row_sum<<<1, 32, 0, st>>>(n, starts, row_sum, out_mean, out_interior);
+}
+void launch_sum_u64(cudaStream_t st, const unsigned long long* v, uint32_t n, unsigned long long* out) {
+    k_sum_u64<<<grid_for(n, 256, 2), 256, 0, st>>>(v, n, out);
+}
+
+void configure_transfer_kernels(int max_dyn_smem) {
+    cudaFuncSetAttribute(k_visibility, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_closure, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+}
+
+}  // namespace ifx

@@ -1,0 +1,140 @@
+// Kernel entry points and their parameter blocks (host <-> device).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "layout.h"
+
+namespace ifx {
+
+struct GatherView;
+
+// Program blob as handed to every tracing kernel. When `staged` is set the
+// kernel copies it into dynamic shared memory (bytes of it); otherwise it
+// reads it from global memory (large scenes).
+struct BlobRef {
+    const uint8_t* ptr;
+    uint32_t bytes;
+    int staged;
+};
+
+struct CamParams {
+    float origin[3], fwd[3], right[3], up[3];
+    float tan_half, aspect;
+};
+
+struct GridParams {
+    const float4* gp;
+    const float4* gn;
+    const float4* girr;
+    const uint32_t* starts;
+    int dim[3];
+    float lo[3];
+    float inv_cell;
+    float radius;
+};
+
+// Surfel state, structure of arrays, 16 bytes per field per surfel.
+struct SurfelArrays {
+    float4* p;       // xyz, w = area
+    float4* n;       // xyz
+    float4* albedo;  // xyz
+    float4* direct;
+    float4* irr;
+    float4* rad;
+};
+
+// ---- generation (surfel.rs:147-255) ----
+void launch_gen_project(cudaStream_t st, BlobRef blob, SceneConsts sc, uint32_t seed0, uint32_t count, float eps,
+                        float4* out, uint32_t* status);
+void launch_gen_finalize(cudaStream_t st, BlobRef blob, const float4* pts, uint32_t n, float area, SurfelArrays s,
+                         uint32_t* status);
+
+// ---- clusters (formfactor.rs:91-147) ----
+void launch_cluster_keys(cudaStream_t st, const float4* p, const float4* n, uint32_t count, SceneConsts sc,
+                         int res, unsigned long long* keys);
+void launch_seg_heads(cudaStream_t st, const unsigned long long* sorted, uint32_t count, uint32_t* heads);
+void launch_seg_starts(cudaStream_t st, const unsigned long long* sorted, const uint32_t* head_scan,
+                       uint32_t count, uint32_t* seg_start, uint32_t* members);
+void launch_cluster_reduce(cudaStream_t st, const uint32_t* seg_start, const uint32_t* members, uint32_t nseg,
+                           const float4* sp, const float4* sn, float4* cp, float4* cn, uint32_t* valid);
+void launch_cluster_compact(cudaStream_t st, const uint32_t* valid, const uint32_t* valid_scan, uint32_t nseg,
+                            const uint32_t* seg_start, const float4* cp_in, const float4* cn_in, float4* cp,
+                            float4* cn, uint2* crange);
+
+// ---- transfer (formfactor.rs:153-277) ----
+void launch_pair_count(cudaStream_t st, const float4* sp, const float4* sn, uint32_t n, const float4* cp,
+                       const float4* cn, uint32_t nc, unsigned long long* cand_count);
+void launch_pair_fill(cudaStream_t st, const float4* sp, const float4* sn, uint32_t n, const float4* cp,
+                      const float4* cn, uint32_t nc, const unsigned long long* cand_off, uint32_t* cand_c,
+                      float* cand_ff, uint32_t* cand_row);
+void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
+                       const float4* cp, const float4* cn, const uint32_t* cand_c, const uint32_t* cand_row,
+                       unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status);
+void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
+                    uint32_t n, uint32_t* row_open, uint32_t* row_csteps, uint32_t* status);
+void launch_row_finalize(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const float* cand_ff,
+                         const float* cand_vis, const uint8_t* cand_steps, const uint32_t* row_open,
+                         const uint32_t* row_csteps, uint32_t* row_links, float* row_scale, float* row_sum,
+                         float* row_sky, unsigned long long* row_evals);
+void launch_row_fill(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const uint32_t* cand_c,
+                     const float* cand_ff, const float* cand_vis, const float* row_scale, const uint32_t* starts,
+                     uint32_t* idx, float* w);
+// One thread: the f32 mean of the calibrated row sums over rows with links,
+// summed in row order (formfactor.rs:242-253).
+void launch_mean_row_sum(cudaStream_t st, uint32_t n, const uint32_t* starts, const float* row_sum,
+                         float* out_mean, unsigned long long* out_interior);
+void launch_sum_u64(cudaStream_t st, const unsigned long long* v, uint32_t n, unsigned long long* out);
+
+// ---- solve (solve.rs:27-108) ----
+struct SolveCtl {
+    uint32_t done;
+    uint32_t iterations;
+    uint32_t residual_bits;  // max |delta| of the bounce in progress (non-negative f32 bits)
+    uint32_t last_residual;  // residual of the last completed bounce
+};
+void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_t n, unsigned long long* evals,
+                          uint32_t* status);
+void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
+                         const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
+                         const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches);
+
+// ---- grid + shade (surfel.rs:71-114, main.rs:229-367, film.rs:51-61) ----
+void launch_grid_keys(cudaStream_t st, const float4* p, uint32_t n, GridParams g, unsigned long long* keys);
+void launch_grid_starts(cudaStream_t st, const unsigned long long* sorted, uint32_t n, uint32_t ncells,
+                        uint32_t* starts);
+void launch_grid_scatter(cudaStream_t st, const unsigned long long* sorted, uint32_t n, SurfelArrays s,
+                         float4* gp, float4* gn, float4* girr, uint32_t* items);
+
+struct ShadeParams {
+    BlobRef blob;
+    GridParams grid;
+    int has_gi;
+    CamParams cam;
+    uint32_t w, h;
+    float tmax;
+    int mode;
+    float exposure;
+    int tonemap;
+    const float* srgb_t;  // 256 thresholds
+    float* film;          // w*h*3, nullable
+    uint8_t* out8;        // w*h*3, nullable
+    unsigned long long* evals;
+    uint32_t* status;
+};
+void launch_shade(cudaStream_t st, const ShadeParams& p);
+
+// Raises the dynamic shared-memory limit of every scene-staging kernel.
+void configure_surfel_kernels(int max_dyn_smem);
+void configure_transfer_kernels(int max_dyn_smem);
+void configure_solve_kernels(int max_dyn_smem);
+void configure_shade_kernels(int max_dyn_smem);
+inline void configure_kernels(int max_dyn_smem) {
+    configure_surfel_kernels(max_dyn_smem);
+    configure_transfer_kernels(max_dyn_smem);
+    configure_solve_kernels(max_dyn_smem);
+    configure_shade_kernels(max_dyn_smem);
+}
+
+}  // namespace ifx
