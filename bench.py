@@ -1,0 +1,398 @@
+"""Benchmark: one frame of the surfel-radiosity path on the product-scale scene.
+
+A step is one frame on fixed surfels: transfer build (clusters, candidate
+pairs, visibility, closure, CSR) -> direct light on surfels -> Jacobi solve
+-> gather grid -> per-pixel shade with the sRGB encode, i.e. the stages the
+reference runs after surfel generation (main.rs:448-475 and 522-534). Surfel
+generation runs once before timing and is reported separately.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2_product] [--no-cpu-baseline]
+
+N > 1 runs under torchrun as N independent replicas (one process per GPU,
+each rendering its own frame; the path has no cross-GPU exchange), timed on
+the device and reduced as the max over ranks. `--impl reference` times the
+reference algorithm's CPU implementation (the oracle restatement in oracle/,
+since the Rust reference cannot be built here) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (scene file, description)
+    "c2_product": ("interflect_b200/scenes/c2_product.rad",
+                   "product scale: 5 objects + floor plane, quad + sphere light, 1920x1080, 200k surfels requested, "
+                   "16 bounces"),
+    "c2_product_strict": ("interflect_b200/scenes/c2_product_strict.rad",
+                          "product scale, reference features only"),
+    "c1_cornell": ("interflect_b200/scenes/c1_cornell.rad", "Cornell box 260x260, 20k surfels, 12 bounces"),
+    "c3_stress": ("interflect_b200/scenes/c3_stress.rad",
+                  "512 primitives, 3840x2160, 1M surfels requested, 24 bounces"),
+}
+METRIC = "SDF evaluations per second, one full frame (transfer + light + solve + grid + shade)"
+UNIT = "evals/s"
+FP32_LANES_PER_SM = 128
+N_SMS = 148
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def fp32_peak_tflops(peaks: dict) -> tuple[float, str]:
+    """Non-tensor FP32 peak: 148 SMs x 128 lanes x 2 FLOP (FMA) x max SM clock."""
+    mhz = peaks.get("sm_max_mhz")
+    src = "MEASURED_PEAKS.json sm_max_mhz"
+    if not mhz:
+        mhz, src = 1965.0, "nominal 1965 MHz"
+    return N_SMS * FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12, src
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def allreduce_max_sum(vals_max: list[float], vals_sum: list[float], world: int):
+    if world <= 1:
+        return vals_max, vals_sum
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    tm = torch.tensor(vals_max, dtype=torch.float64, device=dev)
+    ts = torch.tensor(vals_sum, dtype=torch.float64, device=dev)
+    dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+    dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+    return tm.tolist(), ts.tolist()
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class L2Flusher:
+    """Writes a buffer larger than the 126 MB L2 between timed steps."""
+
+    def __init__(self, device: int):
+        import torch
+        self.torch = torch
+        self.buf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+
+    def flush(self):
+        self.buf.fill_(1)
+        self.torch.cuda.synchronize()
+
+
+def frame(ctx, cfg, cluster_res=8):
+    info = ctx.build(cluster_res)
+    le = ctx.light_surfels()
+    st = ctx.solve(cfg.bounces)
+    ctx.grid_build()
+    _, _, se = ctx.render_frame(cfg.width, cfg.height, linear=False, srgb=False)
+    return info, le, st, se
+
+
+def run_ours(args, world, rank, local) -> dict | None:
+    import numpy as np
+    import interflect_b200 as ifx
+
+    scene_path, desc = WORKLOADS[args.workload]
+    with open(os.path.join(ROOT, scene_path)) as f:
+        src = f.read()
+    scene = ifx.parse(src)
+    cfg = scene.cfg
+    ctx = ifx.Context(local)
+    ctx.upload(scene)
+    t0 = time.time()
+    placed = ctx.generate(cfg.surfels)
+    gen_s = time.time() - t0
+    surf = ctx.surfels()
+
+    # Work accounting (instrumented kernels, outside any timed region).
+    ctx.set_work_counting(True)
+    ctx.reset_work()
+    frame(ctx, cfg)
+    work = {k: ctx.work(k) for k in ("visibility", "closure", "light", "shade")}
+    ctx.set_work_counting(False)
+
+    flusher = L2Flusher(local)
+    for _ in range(args.warmup):
+        frame(ctx, cfg)
+    barrier(world)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    launches0 = ctx.stats()["kernel_launches"]
+    total_ms, evals_total = 0.0, 0
+    kms = {"visibility": [], "closure": [], "light": [], "shade": []}
+    stage = {"transfer": [], "light": [], "solve": [], "grid": [], "shade": []}
+    info = st = None
+    for _ in range(args.steps):
+        flusher.flush()
+        ctx.timer_start()
+        info, le, st, se = frame(ctx, cfg)
+        total_ms += ctx.timer_stop()
+        evals_total += info.evals + le + se
+        s = ctx.stats()
+        kms["visibility"].append(s["ms_visibility"])
+        kms["closure"].append(s["ms_closure"])
+        kms["light"].append(s["ms_light"])
+        kms["shade"].append(s["ms_shade"])
+        for k in stage:
+            stage[k].append(s["ms_" + k])
+    launches = ctx.stats()["kernel_launches"] - launches0
+    clocks = sampler.stop() if sampler else None
+    barrier(world)
+
+    # End to end through the C ABI with host buffers: scene + surfels in,
+    # encoded image out, every step.
+    e2e_ms, e2e_evals = 0.0, 0
+    img = np.zeros((cfg.height, cfg.width, 3), np.uint8)
+    h2d = None
+    for i in range(args.warmup + args.steps):
+        flusher.flush()
+        ctx.timer_start()
+        ctx.upload(scene)
+        ctx.upload_surfels(surf["p"], surf["n"], surf["albedo"], surf["area"])
+        info2 = ctx.build(8)
+        le2 = ctx.light_surfels()
+        ctx.solve(cfg.bounces)
+        ctx.grid_build()
+        _, out8, se2 = ctx.render_frame(cfg.width, cfg.height, linear=False, srgb=True)
+        ms = ctx.timer_stop()
+        if i >= args.warmup:
+            e2e_ms += ms
+            e2e_evals += info2.evals + le2 + se2
+            img = out8
+    h2d = placed * 16 * 3 + len(src)  # surfel p+area, n, albedo as float4; scene text
+    d2h = int(img.nbytes)
+
+    (t_max, e2e_max), (ev_sum, e2e_ev_sum) = allreduce_max_sum([total_ms, e2e_ms], [evals_total, e2e_evals], world)
+    if rank != 0:
+        return None
+
+    sec = t_max / 1e3
+    value = ev_sum / sec
+    # Dominant kernel: the one with the largest share of the frame.
+    avg = {k: statistics.mean(v) for k, v in kms.items()}
+    dom = max(avg, key=avg.get)
+    flops = work[dom][1]
+    peaks = measured_peaks()
+    peak, peak_src = fp32_peak_tflops(peaks)
+    achieved = flops / (avg[dom] / 1e3) / 1e12
+    traffic = None
+    tj = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tj):
+        with open(tj) as f:
+            traffic = json.load(f).get(args.workload, {}).get(dom)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "scene": scene_path, "description": desc,
+                   "film": [cfg.width, cfg.height], "surfels_requested": cfg.surfels, "surfels_placed": placed,
+                   "clusters": info.clusters, "candidates": info.candidates, "links": info.links,
+                   "bounces_run": st.iterations, "max_bounces": cfg.bounces,
+                   "evals_per_frame": evals_total // max(args.steps, 1),
+                   "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
+        "frame_ms": t_max / args.steps,
+        "stage_ms": {k: statistics.mean(v) for k, v in stage.items()},
+        "kernel_ms": avg,
+        "surfel_generation_s": gen_s,
+        "roofline": {"kernel": dom, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "flops_per_launch": flops, "peak_source": f"fp32 CUDA-core peak from {peak_src}",
+                     "work": {k: float(v[1]) for k, v in work.items()}},
+        "e2e": {"value": e2e_ev_sum / (e2e_max / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_max / args.steps},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(src, surf, cfg, args)
+    return line
+
+
+def cpu_frame(src, surf, cfg, threads, rows_frac=1.0):
+    """One frame of the oracle (the reference algorithm on the CPU) on the
+    given surfels; shading restricted to the first rows_frac of the rows."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Oracle
+    o = Oracle(src, threads=threads)
+    o.set_surfels(surf["p"], surf["n"], surf["albedo"], surf["area"])
+    t0 = time.perf_counter()
+    o.build_clusters(8)
+    info = o.build_transfer()
+    le = o.light_surfels()
+    o.solve(cfg.bounces)
+    o.build_grid()
+    rows = max(1, int(cfg.height * rows_frac))
+    _, se = o.render(cfg.width, cfg.height, "beauty", rows=(0, rows))
+    dt = time.perf_counter() - t0
+    return info["evals"] + le + se, dt, rows
+
+
+def cpu_baseline(src, surf, cfg, args) -> dict:
+    threads = os.cpu_count() or 1
+    ev, dt, rows = cpu_frame(src, surf, cfg, threads, rows_frac=args.cpu_rows)
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one frame of the same workload on the same surfels, shading rows 0..{rows} of "
+                      f"{cfg.height}; {ev / 1e6:.1f}M SDF evals in {dt:.2f} s",
+            "cpu": cpu_model()}
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args, world, rank) -> dict | None:
+    if rank != 0:
+        return None
+    import interflect_b200  # noqa: F401  (scene parsing only)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Oracle
+    scene_path, desc = WORKLOADS[args.workload]
+    with open(os.path.join(ROOT, scene_path)) as f:
+        src = f.read()
+    threads = os.cpu_count() or 1
+    o = Oracle(src, threads=threads)
+    cfg_i = o.info()
+    t0 = time.time()
+    placed = o.generate(cfg_i["surfels"])
+    gen_s = time.time() - t0
+    surf = o.surfels()
+
+    class Cfg:
+        width, height, bounces = cfg_i["width"], cfg_i["height"], cfg_i["bounces"]
+    total_t, total_ev, rows = 0.0, 0, cfg_i["height"]
+    for i in range(args.warmup + args.steps):
+        ev, dt, rows = cpu_frame(src, surf, Cfg, threads, rows_frac=args.cpu_rows)
+        if i >= args.warmup:
+            total_t += dt
+            total_ev += ev
+    value = total_ev / total_t
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_t / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "scene": scene_path, "description": desc,
+                       "surfels_placed": placed, "film": [cfg_i["width"], cfg_i["height"]]},
+            "surfel_generation_s": gen_s,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} frames on the host cores, shading rows 0..{rows} of "
+                                       f"{cfg_i['height']}", "cpu": cpu_model()},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the Rust reference cannot be built in this image (no rustc/cargo); this arm times the "
+                    "oracle, a line-by-line C++ restatement of the reference's CPU path, on all host threads"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2_product", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-rows", type=float, default=1.0, help="fraction of film rows the CPU legs shade")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_setup()
+    try:
+        line = run_reference(args, world, rank) if args.impl == "reference" else run_ours(args, world, rank, local)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

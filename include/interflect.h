@@ -101,7 +101,15 @@ typedef struct ifx_solve_stats {
 typedef struct ifx_stats {
     uint64_t kernel_launches;  /* kernels this context has launched so far */
     float ms_transfer, ms_light, ms_solve, ms_grid, ms_shade; /* CUDA-event times of the last call of each stage */
+    float ms_visibility, ms_closure; /* CUDA-event times of the last visibility and closure kernels */
 } ifx_stats;
+
+/* Tracing kernels, for work accounting. */
+#define IFX_KERNEL_VISIBILITY 0
+#define IFX_KERNEL_CLOSURE 1
+#define IFX_KERNEL_LIGHT 2
+#define IFX_KERNEL_SHADE 3
+#define IFX_WORK_COUNTERS 21
 
 /* ------------------------------------------------------------- scene --- */
 
@@ -128,6 +136,21 @@ int ifx_ctx_create(int device, ifx_ctx** out);
 void ifx_ctx_destroy(ifx_ctx* ctx);
 const char* ifx_last_error(const ifx_ctx* ctx);
 int ifx_get_stats(const ifx_ctx* ctx, ifx_stats* out);
+
+/* Measurement support (no reference counterpart). While counting is on, the
+ * tracing kernels run an instrumented instantiation (slower; never use it for
+ * timing) that tallies their work per kernel: node tests, primitive
+ * evaluations by kind, march steps, form factors, gather items.
+ * ifx_get_work returns the tallies (IFX_WORK_COUNTERS u64) of one kernel and
+ * their algorithmic FLOPs under the library's FLOP model; ifx_reset_work
+ * clears them. */
+int ifx_set_work_counting(ifx_ctx* ctx, int on);
+int ifx_reset_work(ifx_ctx* ctx);
+int ifx_get_work(ifx_ctx* ctx, int kernel, uint64_t* counts, double* flops);
+
+/* CUDA events on the context's stream around caller-chosen work. */
+int ifx_timer_start(ifx_ctx* ctx);
+int ifx_timer_stop(ifx_ctx* ctx, float* ms);
 
 /* Flattens the scene (SDF object program, BVH nodes, planes, lights,
  * materials) into device memory. Must precede every stage below. */

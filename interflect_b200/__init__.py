@@ -42,7 +42,10 @@ EXPORTS = (
     "ifx_surfels_generate", "ifx_surfels_upload", "ifx_surfels_count", "ifx_surfels_download",
     "ifx_transfer_build", "ifx_transfer_download", "ifx_clusters_download", "ifx_transfer_row_diag",
     "ifx_transfer_upload", "ifx_light_surfels", "ifx_solve", "ifx_grid_build", "ifx_render_frame",
+    "ifx_set_work_counting", "ifx_reset_work", "ifx_get_work", "ifx_timer_start", "ifx_timer_stop",
 )
+KERNELS = {"visibility": 0, "closure": 1, "light": 2, "shade": 3}
+WORK_COUNTERS = 21
 
 
 class ParseError(ValueError):
@@ -84,7 +87,8 @@ class _SolveStats(C.Structure):
 
 class _Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_uint64), ("ms_transfer", C.c_float), ("ms_light", C.c_float),
-                ("ms_solve", C.c_float), ("ms_grid", C.c_float), ("ms_shade", C.c_float)]
+                ("ms_solve", C.c_float), ("ms_grid", C.c_float), ("ms_shade", C.c_float),
+                ("ms_visibility", C.c_float), ("ms_closure", C.c_float)]
 
 
 _lib_handle = None
@@ -124,6 +128,11 @@ def lib() -> C.CDLL:
         "ifx_solve": (I, [P, U32, C.POINTER(_SolveStats)]),
         "ifx_grid_build": (I, [P, F]),
         "ifx_render_frame": (I, [P, C.POINTER(_Camera), I, U32, U32, F, P, P, C.POINTER(U64)]),
+        "ifx_set_work_counting": (I, [P, I]),
+        "ifx_reset_work": (I, [P]),
+        "ifx_get_work": (I, [P, I, P, C.POINTER(C.c_double)]),
+        "ifx_timer_start": (I, [P]),
+        "ifx_timer_stop": (I, [P, C.POINTER(F)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -395,6 +404,28 @@ class Context:
         s = _Stats()
         lib().ifx_get_stats(self._h, C.byref(s))
         return {f: getattr(s, f) for f, _ in _Stats._fields_}
+
+    # -- measurement ----------------------------------------------------------
+    def set_work_counting(self, on: bool) -> None:
+        """Instrumented kernels (for work/FLOP accounting only, never for timing)."""
+        self._check(lib().ifx_set_work_counting(self._h, 1 if on else 0), "set_work_counting")
+
+    def reset_work(self) -> None:
+        self._check(lib().ifx_reset_work(self._h), "reset_work")
+
+    def work(self, kernel: str) -> tuple[np.ndarray, float]:
+        counts = np.zeros(WORK_COUNTERS, np.uint64)
+        fl = C.c_double()
+        self._check(lib().ifx_get_work(self._h, KERNELS[kernel], _ptr(counts), C.byref(fl)), "get_work")
+        return counts, fl.value
+
+    def timer_start(self) -> None:
+        self._check(lib().ifx_timer_start(self._h), "timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        self._check(lib().ifx_timer_stop(self._h, C.byref(ms)), "timer_stop")
+        return ms.value
 
 
 def cuda_available() -> bool:

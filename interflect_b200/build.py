@@ -27,7 +27,7 @@ CLI = os.path.join(HERE, "bin", "interflect")
 
 CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "capi.cu"]
 CPP_SOURCES = ["scene_host.cpp"]
-HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh"]
+HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh", "flop_model.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",

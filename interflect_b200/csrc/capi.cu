@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/interflect.h"
+#include "flop_model.h"
 #include "kernels.h"
 #include "scene_host.h"
 
@@ -80,6 +81,17 @@ struct ifx_ctx {
     DBuf cub_tmp, small;  // small: 8 x u64 counters / results
     DBuf gen_cand;
     std::vector<float4> gen_host;
+
+    // measurement: per-kernel events, work counters (4 kernels x 21 u64), timer
+    cudaEvent_t kv0 = nullptr, kv1 = nullptr, kc0 = nullptr, kc1 = nullptr, tm0 = nullptr, tm1 = nullptr;
+    bool counting = false;
+    DBuf work;
+    void* pinned = nullptr;  // upload staging (page-locked)
+    size_t pinned_cap = 0;
+
+    unsigned long long* work_of(int kernel) {
+        return counting ? (unsigned long long*)work.p + (size_t)kernel * IFX_WORK_COUNTERS : nullptr;
+    }
 
     SurfelArrays sarr() {
         return SurfelArrays{(float4*)sp.p, (float4*)sn.p, (float4*)salb.p, (float4*)sdir.p, (float4*)sirr.p,
@@ -276,6 +288,11 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
     if ((e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) return bail(e);
+    for (cudaEvent_t* ev : {&ctx->kv0, &ctx->kv1, &ctx->kc0, &ctx->kc1, &ctx->tm0, &ctx->tm1})
+        if ((e = cudaEventCreate(ev)) != cudaSuccess) return bail(e);
+    if (ensure(ctx, ctx->work, 4 * IFX_WORK_COUNTERS * 8) != IFX_OK ||
+        cudaMemsetAsync(ctx->work.p, 0, 4 * IFX_WORK_COUNTERS * 8, ctx->st) != cudaSuccess)
+        return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->status, 16) != IFX_OK || ensure(ctx, ctx->small, 64) != IFX_OK ||
         ensure(ctx, ctx->srgb_t, 256 * sizeof(float)) != IFX_OK || ensure(ctx, ctx->ctl, sizeof(SolveCtl)) != IFX_OK)
         return bail(cudaErrorMemoryAllocation);
@@ -302,10 +319,11 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->row_scale, &ctx->row_sum, &ctx->row_sky, &ctx->row_evals, &ctx->starts, &ctx->idx,
                     &ctx->w, &ctx->cluster_rad, &ctx->ctl, &ctx->gkeys, &ctx->gkeys_alt, &ctx->gstarts, &ctx->gp,
                     &ctx->gn, &ctx->girr, &ctx->gitems, &ctx->film, &ctx->out8, &ctx->cub_tmp, &ctx->small,
-                    &ctx->gen_cand};
+                    &ctx->gen_cand, &ctx->work};
     for (DBuf* b : bufs) free_buf(*b);
-    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
-    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
+        if (ev) cudaEventDestroy(ev);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }
@@ -316,6 +334,48 @@ extern "C" int ifx_get_stats(const ifx_ctx* ctx, ifx_stats* out) {
     if (!ctx || !out) return IFX_ERR_INVALID;
     *out = ctx->stats;
     out->kernel_launches = ctx->launches;
+    return IFX_OK;
+}
+
+extern "C" int ifx_set_work_counting(ifx_ctx* ctx, int on) {
+    if (!ctx) return IFX_ERR_INVALID;
+    ctx->counting = on != 0;
+    return IFX_OK;
+}
+
+extern "C" int ifx_reset_work(ifx_ctx* ctx) {
+    if (!ctx) return IFX_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemsetAsync(ctx->work.p, 0, 4 * IFX_WORK_COUNTERS * 8, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return IFX_OK;
+}
+
+extern "C" int ifx_get_work(ifx_ctx* ctx, int kernel, uint64_t* counts, double* flops) {
+    if (!ctx || kernel < 0 || kernel > 3) return fail(ctx, IFX_ERR_INVALID, "bad kernel id");
+    CK(cudaSetDevice(ctx->device));
+    unsigned long long h[IFX_WORK_COUNTERS];
+    CK(cudaMemcpyAsync(h, (unsigned long long*)ctx->work.p + (size_t)kernel * IFX_WORK_COUNTERS, sizeof h,
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (counts) memcpy(counts, h, sizeof h);
+    if (flops) *flops = work_flops(h, IFX_WORK_COUNTERS);
+    return IFX_OK;
+}
+
+extern "C" int ifx_timer_start(ifx_ctx* ctx) {
+    if (!ctx) return IFX_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventRecord(ctx->tm0, ctx->st));
+    return IFX_OK;
+}
+
+extern "C" int ifx_timer_stop(ifx_ctx* ctx, float* ms) {
+    if (!ctx || !ms) return IFX_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventRecord(ctx->tm1, ctx->st));
+    CK(cudaEventSynchronize(ctx->tm1));
+    CK(cudaEventElapsedTime(ms, ctx->tm0, ctx->tm1));
     return IFX_OK;
 }
 
@@ -359,13 +419,23 @@ extern "C" int ifx_surfels_upload(ifx_ctx* ctx, uint64_t n, const float* p, cons
     if (!ctx || (n && (!p || !nrm || !albedo || !area))) return fail(ctx, IFX_ERR_INVALID, "null argument");
     if (n > 2000000ull) return fail(ctx, IFX_ERR_LIMIT, "more than 2000000 surfels");
     CK(cudaSetDevice(ctx->device));
-    std::vector<float4> hp(n), hn(n), ha(n);
+    size_t b = n * sizeof(float4);
+    // Repack into the device layout in pinned staging memory, then copy.
+    if (ctx->pinned_cap < 3 * b) {
+        if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        ctx->pinned = nullptr;
+        ctx->pinned_cap = 0;
+        CK(cudaHostAlloc(&ctx->pinned, 3 * b, cudaHostAllocDefault));
+        ctx->pinned_cap = 3 * b;
+    }
+    float4* hp = (float4*)ctx->pinned;
+    float4* hn = hp + n;
+    float4* ha = hn + n;
     for (uint64_t i = 0; i < n; ++i) {
         hp[i] = make_float4(p[3 * i], p[3 * i + 1], p[3 * i + 2], area[i]);
         hn[i] = make_float4(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2], 0.0f);
         ha[i] = make_float4(albedo[3 * i], albedo[3 * i + 1], albedo[3 * i + 2], 0.0f);
     }
-    size_t b = n * sizeof(float4);
     ENSURE(ctx->sp, b);
     ENSURE(ctx->sn, b);
     ENSURE(ctx->salb, b);
@@ -373,9 +443,9 @@ extern "C" int ifx_surfels_upload(ifx_ctx* ctx, uint64_t n, const float* p, cons
     ENSURE(ctx->sirr, b);
     ENSURE(ctx->srad, b);
     if (n) {
-        CK(cudaMemcpyAsync(ctx->sp.p, hp.data(), b, cudaMemcpyHostToDevice, ctx->st));
-        CK(cudaMemcpyAsync(ctx->sn.p, hn.data(), b, cudaMemcpyHostToDevice, ctx->st));
-        CK(cudaMemcpyAsync(ctx->salb.p, ha.data(), b, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->sp.p, hp, b, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->sn.p, hn, b, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->salb.p, ha, b, cudaMemcpyHostToDevice, ctx->st));
         CK(cudaMemsetAsync(ctx->sdir.p, 0, b, ctx->st));
         CK(cudaMemsetAsync(ctx->sirr.p, 0, b, ctx->st));
         CK(cudaMemsetAsync(ctx->srad.p, 0, b, ctx->st));
@@ -629,17 +699,21 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     CKL();
 
     // Visibility and closure.
-    launch_visibility(ctx->st, ctx->blobref, ctx->sc, sp, sn, cp, cn, (const uint32_t*)ctx->cand_c.p,
-                      (const uint32_t*)ctx->cand_row.p, ncand, (float*)ctx->cand_vis.p,
-                      (uint8_t*)ctx->cand_steps.p, status);
-    if (ncand) ctx->launches++;
-    CKL();
     ENSURE(ctx->row_open, (size_t)n * 4);
     ENSURE(ctx->row_csteps, (size_t)n * 4);
+    CK(cudaEventRecord(ctx->kv0, ctx->st));
+    launch_visibility(ctx->st, ctx->blobref, ctx->sc, sp, sn, cp, cn, (const uint32_t*)ctx->cand_c.p,
+                      (const uint32_t*)ctx->cand_row.p, ncand, (float*)ctx->cand_vis.p,
+                      (uint8_t*)ctx->cand_steps.p, status, ctx->work_of(IFX_KERNEL_VISIBILITY));
+    if (ncand) ctx->launches++;
+    CKL();
+    CK(cudaEventRecord(ctx->kv1, ctx->st));
+    CK(cudaEventRecord(ctx->kc0, ctx->st));
     launch_closure(ctx->st, ctx->blobref, ctx->sc, sp, sn, n, (uint32_t*)ctx->row_open.p,
-                   (uint32_t*)ctx->row_csteps.p, status);
+                   (uint32_t*)ctx->row_csteps.p, status, ctx->work_of(IFX_KERNEL_CLOSURE));
     ctx->launches++;
     CKL();
+    CK(cudaEventRecord(ctx->kc1, ctx->st));
 
     // Rows: links, ordered sums, calibration, CSR.
     ENSURE(ctx->row_links, ((size_t)n + 1) * 4);
@@ -686,6 +760,8 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->stats.ms_transfer = ms;
+    CK(cudaEventElapsedTime(&ctx->stats.ms_visibility, ctx->kv0, ctx->kv1));
+    CK(cudaEventElapsedTime(&ctx->stats.ms_closure, ctx->kc0, ctx->kc1));
     ctx->ncand = ncand;
     ctx->links = links;
     ctx->has_transfer = true;
@@ -790,7 +866,8 @@ extern "C" int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals) {
     CK(cudaMemsetAsync(small, 0, 8, ctx->st));
     CK(cudaEventRecord(ctx->ev0, ctx->st));
     if (ctx->n) {
-        launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), ctx->n, small, (uint32_t*)ctx->status.p);
+        launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), ctx->n, small, (uint32_t*)ctx->status.p,
+                             ctx->work_of(IFX_KERNEL_LIGHT));
         ctx->launches++;
         CKL();
     }
@@ -948,13 +1025,14 @@ extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, u
         ENSURE(ctx->film, px * 12);
         P.film = (float*)ctx->film.p;
     }
-    if (out_srgb) {
-        ENSURE(ctx->out8, px * 3);
-        P.out8 = (uint8_t*)ctx->out8.p;
-    }
+    // The encoded frame always lands in device memory; it is copied out only
+    // when the caller asks for it.
+    ENSURE(ctx->out8, px * 3);
+    P.out8 = (uint8_t*)ctx->out8.p;
     unsigned long long* small = (unsigned long long*)ctx->small.p;
     P.evals = &small[3];
     P.status = (uint32_t*)ctx->status.p;
+    P.counts = ctx->work_of(IFX_KERNEL_SHADE);
     CK(cudaMemsetAsync(&small[3], 0, 8, ctx->st));
     CK(cudaEventRecord(ctx->ev0, ctx->st));
     launch_shade(ctx->st, P);

@@ -3,7 +3,7 @@
 // gather. Every function keeps the reference's f32 operation order; the
 // library is compiled with --fmad=false and IEEE division/square root, so
 // each result is bit-identical to the unfused f32 arithmetic of the
-// reference (transcendentals excepted: acosf comes from CUDA's libdevice).
+// reference (acos reproduces glibc's acosf exactly; only the sphere-light extension calls CUDA's atanf).
 #pragma once
 
 #include <cstdint>
@@ -89,6 +89,53 @@ __device__ __forceinline__ SceneView make_view(const uint8_t* base) {
 static constexpr uint32_t kStatusStageTimeout = 1u;
 static constexpr uint32_t kStatusStackOverflow = 2u;
 
+// ------------------------------------------------------- work counters ----
+// Tracing functions take a counter policy. NoCount compiles to nothing and is
+// what the timed kernels use; Counts tallies the work of one thread so that
+// a separate counting launch can derive the algorithmic FLOPs of a kernel
+// (the per-item costs are in flop_model.h).
+enum CounterId : int {
+    CN_NODE = 0,       // BVH aabb_dist evaluations
+    CN_PRIM = 1,       // CN_PRIM + kind: primitive distance evaluations (8 kinds)
+    CN_SMOOTH = 9,     // smooth subtractions
+    CN_HARD = 10,      // hard subtractions max(d, -s)
+    CN_SDF = 11,       // scene distance queries
+    CN_TSTEP = 12,     // sphere-tracing steps
+    CN_SSTEP = 13,     // soft-shadow steps
+    CN_FF = 14,        // quad form factors
+    CN_FF_EDGE = 15,   // edges summed by quad form factors
+    CN_LIGHT = 16,     // light evaluations past the form-factor cull
+    CN_SPEC = 17,      // specular lobes
+    CN_GVISIT = 18,    // surfels visited by gather
+    CN_GACCEPT = 19,   // surfels accumulated by gather
+    CN_SSTEP_HIT = 20, // (reserved)
+    kNumCounters = 21
+};
+
+struct NoCount {
+    __device__ __forceinline__ void add(int, uint32_t = 1) {}
+};
+
+struct Counts {
+    uint32_t v[kNumCounters];
+    __device__ __forceinline__ Counts() {
+#pragma unroll
+        for (int i = 0; i < kNumCounters; ++i) v[i] = 0;
+    }
+    __device__ __forceinline__ void add(int id, uint32_t k = 1) { v[id] += k; }
+    // Warp-level sum, then one 64-bit atomic per counter per warp (integer,
+    // so the totals do not depend on scheduling). All lanes must call.
+    __device__ __forceinline__ void flush(unsigned long long* out) {
+#pragma unroll 1
+        for (int i = 0; i < kNumCounters; ++i) {
+            unsigned long long x = v[i];
+            for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if ((threadIdx.x & 31) == 0 && x) atomicAdd(&out[i], x);
+            v[i] = 0;
+        }
+    }
+};
+
 // Copies the program blob into dynamic shared memory with one bulk
 // (non-multicast) async copy completed on an mbarrier, and returns a view of
 // it. The wait is bounded: on expiry the status word gets
@@ -131,9 +178,11 @@ __device__ __forceinline__ bool stage_scene(const uint8_t* gblob, uint32_t bytes
 
 // ------------------------------------------------------------- sdf.rs -----
 // sdf.rs:52-125 over a packed primitive (hoisted terms in layout.h).
-__device__ __forceinline__ float prim_dist(const DPrim& pr, V p) {
+template <class C>
+__device__ __forceinline__ float prim_dist(const DPrim& pr, V p, C& cnt) {
     const float4* q = reinterpret_cast<const float4*>(&pr);
     const int kind = pr.kind;
+    cnt.add(CN_PRIM + kind);
     const float4 a = q[1];
     switch (kind) {
         case K_SPHERE:
@@ -204,10 +253,12 @@ __device__ __forceinline__ float prim_dist(const DPrim& pr, V p) {
 }
 
 // sdf.rs:166-172 with the smooth-subtraction extension.
-__device__ __forceinline__ float obj_dist(const SceneView& sv, const DObject& o, V p) {
-    float d = prim_dist(sv.prims[o.prim], p);
+template <class C>
+__device__ __forceinline__ float obj_dist(const SceneView& sv, const DObject& o, V p, C& cnt) {
+    float d = prim_dist(sv.prims[o.prim], p, cnt);
     for (int s = 1; s <= o.nsub; ++s) {
-        float sd = prim_dist(sv.prims[o.prim + s], p);
+        float sd = prim_dist(sv.prims[o.prim + s], p, cnt);
+        cnt.add(o.smooth > 0.0f ? CN_SMOOTH : CN_HARD);
         if (o.smooth > 0.0f) {
             float k = o.smooth;
             float hk = clampr(0.5f - 0.5f * (d + sd) / k, 0.0f, 1.0f);
@@ -220,7 +271,9 @@ __device__ __forceinline__ float obj_dist(const SceneView& sv, const DObject& o,
 }
 
 // bvh.rs:46-50
-__device__ __forceinline__ float aabb_dist(V p, const DNode& n) {
+template <class C>
+__device__ __forceinline__ float aabb_dist(V p, const DNode& n, C& cnt) {
+    cnt.add(CN_NODE);
     V lo{n.lo[0], n.lo[1], n.lo[2]}, hi{n.hi[0], n.hi[1], n.hi[2]};
     return len(vmax(vmax(lo - p, p - hi), V{0.0f, 0.0f, 0.0f}));
 }
@@ -231,11 +284,13 @@ struct DistHit {
 };
 
 // scene.rs:191-208 with bvh.rs:100-150 (query) or bvh.rs:155-163 (linear).
-__device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p) {
+template <class C>
+__device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
+    cnt.add(CN_SDF);
     DistHit best{kMaxF, 0u};
     for (int i = 0; i < sv.n_planes; ++i) {
         const DObject o = sv.objs[i];
-        float d = obj_dist(sv, o, p);
+        float d = obj_dist(sv, o, p, cnt);
         if (d < best.d) best = DistHit{d, o.mat};
     }
     if (sv.use_bvh) {
@@ -246,11 +301,11 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p) {
         while (sp > 0) {
             const int ni = stack[--sp];
             const DNode nd = sv.nodes[ni];
-            if (aabb_dist(p, nd) >= best.d) continue;
+            if (aabb_dist(p, nd, cnt) >= best.d) continue;
             if (nd.count > 0) {
                 for (int k = nd.link; k < nd.link + nd.count; ++k) {
                     const DObject o = sv.objs[k];
-                    float d = obj_dist(sv, o, p);
+                    float d = obj_dist(sv, o, p, cnt);
                     if (d < best.d) {
                         best.d = d;
                         best.mat = o.mat;
@@ -258,8 +313,8 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p) {
                 }
             } else {
                 const int l = ni + 1, r = nd.link;
-                float dl = aabb_dist(p, sv.nodes[l]);
-                float dr = aabb_dist(p, sv.nodes[r]);
+                float dl = aabb_dist(p, sv.nodes[l], cnt);
+                float dr = aabb_dist(p, sv.nodes[r], cnt);
                 // The stack holds 64 entries like the reference's; a BVH
                 // needs depth + 1, far below that for any scene the parser
                 // accepts (the host rejects deeper trees).
@@ -275,7 +330,7 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p) {
     } else {
         for (int k = 0; k < sv.n_objects; ++k) {
             const DObject o = sv.objs[sv.linear[k]];
-            float d = obj_dist(sv, o, p);
+            float d = obj_dist(sv, o, p, cnt);
             if (d < best.d) {
                 best.d = d;
                 best.mat = o.mat;
@@ -285,15 +340,19 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p) {
     return best;
 }
 
-__device__ __forceinline__ float scene_dist(const SceneView& sv, V p) { return dist_mat(sv, p).d; }
+template <class C>
+__device__ __forceinline__ float scene_dist(const SceneView& sv, V p, C& cnt) {
+    return dist_mat(sv, p, cnt).d;
+}
 
 // scene.rs:218-236: tetrahedron taps K = (1,-1,-1), (-1,-1,1), (-1,1,-1), (1,1,1).
-__device__ __forceinline__ V scene_normal(const SceneView& sv, V p) {
+template <class C>
+__device__ __forceinline__ V scene_normal(const SceneView& sv, V p, C& cnt) {
     const float H = 5e-4f;
     V n{0.0f, 0.0f, 0.0f};
     const V K[4] = {V{1.0f, -1.0f, -1.0f}, V{-1.0f, -1.0f, 1.0f}, V{-1.0f, 1.0f, -1.0f}, V{1.0f, 1.0f, 1.0f}};
 #pragma unroll
-    for (int i = 0; i < 4; ++i) n = n + K[i] * scene_dist(sv, p + K[i] * H);
+    for (int i = 0; i < 4; ++i) n = n + K[i] * scene_dist(sv, p + K[i] * H, cnt);
     float l = len(n);
     if (l > 1e-12f) return n / l;
     return V{0.0f, 1.0f, 0.0f};
@@ -313,12 +372,14 @@ struct TraceHit {
 
 // trace.rs:27-58 without the normal; callers that need it call
 // scene_normal(hit.p), which costs exactly the four counted taps.
-__device__ __forceinline__ TraceHit trace(const SceneView& sv, V ro, V rd, float tmin, float tmax) {
+template <class C>
+__device__ __forceinline__ TraceHit trace(const SceneView& sv, V ro, V rd, float tmin, float tmax, C& cnt) {
     float t = tmin;
     uint32_t steps = 0;
     while (steps < kMaxSteps) {
         V p = ro + rd * t;
-        DistHit h = dist_mat(sv, p);
+        DistHit h = dist_mat(sv, p, cnt);
+        cnt.add(CN_TSTEP);
         steps += 1;
         float eps = 1e-4f * fmaxf(t, 1.0f);
         if (h.d < eps) return TraceHit{true, t, p, h.mat, steps + 4};
@@ -329,14 +390,16 @@ __device__ __forceinline__ TraceHit trace(const SceneView& sv, V ro, V rd, float
 }
 
 // trace.rs:84-124
+template <class C>
 __device__ __forceinline__ float soft_shadow(const SceneView& sv, V ro, V rd, float tmin, float tmax, float k,
-                                             uint32_t& steps_out) {
+                                             uint32_t& steps_out, C& cnt) {
     float res = 1.0f;
     float t = tmin;
     uint32_t steps = 0;
     float ph = 1e20f;
     while (steps < kShadowSteps && t < tmax) {
-        float h = scene_dist(sv, ro + rd * t);
+        float h = scene_dist(sv, ro + rd * t, cnt);
+        cnt.add(CN_SSTEP);
         steps += 1;
         if (h < 1e-4f) {
             steps_out = steps;
@@ -372,8 +435,45 @@ __device__ __forceinline__ void frame(V n, V& t, V& b) {
 }
 
 // -------------------------------------------------------------- ltc.rs ----
+// acos in f32 by the published fdlibm method (Sun Microsystems, 1993,
+// e_acosf): pi/2 - (x + x*R(x^2)) for |x| < 1/2 and 2*asin(sqrt((1-x)/2))
+// beyond, with R a degree-(6,4) rational approximation and pi/2 split into
+// high and low parts. It is the algorithm of glibc's acosf, which the
+// reference calls through Rust's f32::acos on Linux; evaluated with IEEE f32
+// operations and no FMA it returns glibc's result for every input in
+// [-1, 1] (checked over all 2,130,706,434 of them).
+__device__ __forceinline__ float acos_f32(float x) {
+    const float pi = __uint_as_float(0x40490fdau), pio2_hi = __uint_as_float(0x3fc90fdau),
+                pio2_lo = __uint_as_float(0x33a22168u);
+    const float p0 = __uint_as_float(0x3e2aaaabu), p1 = __uint_as_float(0xbea6b090u),
+                p2 = __uint_as_float(0x3e4e0aa8u), p3 = __uint_as_float(0xbd241146u),
+                p4 = __uint_as_float(0x3a4f7f04u), p5 = __uint_as_float(0x3811ef08u);
+    const float q1 = __uint_as_float(0xc019d139u), q2 = __uint_as_float(0x4001572du),
+                q3 = __uint_as_float(0xbf303361u), q4 = __uint_as_float(0x3d9dc62eu);
+    const uint32_t hx = __float_as_uint(x), ix = hx & 0x7fffffffu;
+    if (ix == 0x3f800000u) return (hx >> 31) ? pi + 2.0f * pio2_lo : 0.0f;
+    if (ix > 0x3f800000u) return (x - x) / (x - x);
+    float z;
+    if (ix < 0x3f000000u) {
+        if (ix <= 0x32800000u) return pio2_hi + pio2_lo;
+        z = x * x;
+    } else {
+        z = ((hx >> 31) ? (1.0f + x) : (1.0f - x)) * 0.5f;
+    }
+    const float p = z * (p0 + z * (p1 + z * (p2 + z * (p3 + z * (p4 + z * p5)))));
+    const float q = 1.0f + z * (q1 + z * (q2 + z * (q3 + z * q4)));
+    const float r = p / q;
+    if (ix < 0x3f000000u) return pio2_hi - (x - (pio2_lo - x * r));
+    const float s = sqrtf(z);
+    if (hx >> 31) return pi - 2.0f * (s + (r * s - pio2_lo));
+    const float df = __uint_as_float(__float_as_uint(s) & 0xfffff000u);
+    const float c = (z - df * df) / (s + df);
+    return 2.0f * (df + (r * s + c));
+}
+
 // ltc.rs:25-83 on a quad already in the local frame.
-__device__ __forceinline__ float quad_form_factor(const V l[4]) {
+template <class C>
+__device__ __forceinline__ float quad_form_factor(const V l[4], C& cnt) {
     V c[5];
     int n = 0;
 #pragma unroll
@@ -387,7 +487,9 @@ __device__ __forceinline__ float quad_form_factor(const V l[4]) {
             c[n++] = a + (b - a) * t;
         }
     }
+    cnt.add(CN_FF);
     if (n < 3) return 0.0f;
+    cnt.add(CN_FF_EDGE, (uint32_t)n);
     for (int i = 0; i < n; ++i) {
         float ln = len(c[i]);
         if (ln > 1e-9f) c[i] = c[i] / ln;
@@ -397,7 +499,7 @@ __device__ __forceinline__ float quad_form_factor(const V l[4]) {
         V a = c[i];
         V b = c[i + 1 == n ? 0 : i + 1];
         float cos_t = clampr(dot(a, b), -1.0f, 1.0f);
-        float theta = acosf(cos_t);
+        float theta = acos_f32(cos_t);
         V cr = cross(a, b);
         float ln = len(cr);
         if (ln > 1e-9f) sum += theta * (cr.z / ln);
@@ -407,14 +509,15 @@ __device__ __forceinline__ float quad_form_factor(const V l[4]) {
 
 // Quad light form factor at (p, n) in the frame (t, b, n): ltc.rs:108-115
 // (to_local with the winding flip) then quad_form_factor.
-__device__ __forceinline__ float quad_light_ff(const DQuadLight& L, V p, V t, V b, V n) {
+template <class C>
+__device__ __forceinline__ float quad_light_ff(const DQuadLight& L, V p, V t, V b, V n, C& cnt) {
     V loc[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         V d = V{L.v[3 - i][0], L.v[3 - i][1], L.v[3 - i][2]} - p;
         loc[i] = V{dot(d, t), dot(d, b), dot(d, n)};
     }
-    return quad_form_factor(loc);
+    return quad_form_factor(loc, cnt);
 }
 
 // Extension: horizon-clipped sphere-light form factor (Snyder 1996 closed
@@ -432,7 +535,7 @@ __device__ __forceinline__ float sphere_light_ff(V p, V n, V c, float r) {
     float sin_t = sqrtf(fmaxf(1.0f - cos_t * cos_t, 0.0f));
     float y = clampr(-x * (cos_t / sin_t), -1.0f, 1.0f);
     float sty = sin_t * sqrtf(1.0f - y * y);
-    float ill = (cos_t * acosf(y) - x * sty) * sin_s2 + atanf(sty / x);
+    float ill = (cos_t * acos_f32(y) - x * sty) * sin_s2 + atanf(sty / x);
     return fmaxf(ill, 0.0f) * (1.0f / kPiF);
 }
 
@@ -466,8 +569,10 @@ __device__ __forceinline__ float v_smith(float n_dot_v, float n_dot_l, float alp
 }
 
 // shade.rs:104-121: representative-point GGX lobe.
+template <class C>
 __device__ __forceinline__ void add_specular(V& out, V p, V n, V v, V rep, float radius, float alpha,
-                                             float n_dot_v, V f0, V radiance) {
+                                             float n_dot_v, V f0, V radiance, C& cnt) {
+    cnt.add(CN_SPEC);
     V l = nrm(rep - p);
     float n_dot_l = dot(n, l);
     if (n_dot_l <= 0.0f) return;
@@ -482,7 +587,9 @@ __device__ __forceinline__ void add_specular(V& out, V p, V n, V v, V rep, float
 }
 
 // shade.rs:50-125
-__device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DMaterial& m, uint32_t& steps_out) {
+template <class C>
+__device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DMaterial& m, uint32_t& steps_out,
+                                    C& cnt) {
     V out{0.0f, 0.0f, 0.0f};
     uint32_t steps = 0;
     V tan, bit;
@@ -497,15 +604,16 @@ __device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DM
         V ln{L.normal[0], L.normal[1], L.normal[2]};
         V to_light = lc - p;
         if (dot(ln, -nrm(to_light)) <= 0.0f) continue;
-        float ff = quad_light_ff(L, p, tan, bit, n);
+        float ff = quad_light_ff(L, p, tan, bit, n, cnt);
         if (ff <= 1e-6f) continue;
+        cnt.add(CN_LIGHT);
         float dist = len(to_light);
         float radius = L.center[3];
         float k = clampr(dist / radius, 1.5f, 96.0f);
         V ldir = to_light / dist;
         float shadow_end = fmaxf(dist - radius * 1.25f, 0.05f);
         uint32_t s;
-        float vis = soft_shadow(sv, p + n * 3e-3f, ldir, 0.015f, shadow_end, k, s);
+        float vis = soft_shadow(sv, p + n * 3e-3f, ldir, 0.015f, shadow_end, k, s, cnt);
         steps += s;
         if (vis <= 1e-4f) continue;
         V radiance = V{L.emit[0], L.emit[1], L.emit[2]} * vis;
@@ -517,7 +625,7 @@ __device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DM
             float t = dot(V{L.v[0][0], L.v[0][1], L.v[0][2]} - p, ln) / denom;
             if (t > 0.0f) rep = closest_on_quad(L, p + r * t);
         }
-        add_specular(out, p, n, v, rep, radius, alpha, n_dot_v, f0, radiance);
+        add_specular(out, p, n, v, rep, radius, alpha, n_dot_v, f0, radiance, cnt);
     }
     for (int li = 0; li < sv.n_slights; ++li) {  // extension: sphere lights
         const DSphereLight& L = sv.slights[li];
@@ -525,13 +633,14 @@ __device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DM
         V to_light = c - p;
         float ff = sphere_light_ff(p, n, c, L.c[3]);
         if (ff <= 1e-6f) continue;
+        cnt.add(CN_LIGHT);
         float dist = len(to_light);
         float radius = fmaxf(L.c[3], 1e-4f);
         float k = clampr(dist / radius, 1.5f, 96.0f);
         V ldir = to_light / dist;
         float shadow_end = fmaxf(dist - radius * 1.25f, 0.05f);
         uint32_t s;
-        float vis = soft_shadow(sv, p + n * 3e-3f, ldir, 0.015f, shadow_end, k, s);
+        float vis = soft_shadow(sv, p + n * 3e-3f, ldir, 0.015f, shadow_end, k, s, cnt);
         steps += s;
         if (vis <= 1e-4f) continue;
         V radiance = V{L.emit[0], L.emit[1], L.emit[2]} * vis;
@@ -540,14 +649,15 @@ __device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DM
         V ctr = r * dot(to_light, r) - to_light;
         float cl = len(ctr);
         V rep = p + to_light + ctr * clampr(radius / fmaxf(cl, 1e-9f), 0.0f, 1.0f);
-        add_specular(out, p, n, v, rep, radius, alpha, n_dot_v, f0, radiance);
+        add_specular(out, p, n, v, rep, radius, alpha, n_dot_v, f0, radiance, cnt);
     }
     steps_out = steps;
     return out;
 }
 
 // shade.rs:133-164
-__device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V albedo, uint32_t& steps_out) {
+template <class C>
+__device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V albedo, uint32_t& steps_out, C& cnt) {
     V out{0.0f, 0.0f, 0.0f};
     uint32_t steps = 0;
     V tan, bit;
@@ -558,14 +668,15 @@ __device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V alb
         V ln{L.normal[0], L.normal[1], L.normal[2]};
         V to_light = lc - p;
         if (dot(ln, -nrm(to_light)) <= 0.0f) continue;
-        float ff = quad_light_ff(L, p, tan, bit, n);
+        float ff = quad_light_ff(L, p, tan, bit, n, cnt);
         if (ff <= 1e-6f) continue;
+        cnt.add(CN_LIGHT);
         float dist = len(to_light);
         float radius = L.center[3];
         float k = clampr(dist / radius, 1.5f, 96.0f);
         float shadow_end = fmaxf(dist - radius * 1.25f, 0.05f);
         uint32_t s;
-        float vis = soft_shadow(sv, p + n * 3e-3f, to_light / dist, 0.015f, shadow_end, k, s);
+        float vis = soft_shadow(sv, p + n * 3e-3f, to_light / dist, 0.015f, shadow_end, k, s, cnt);
         steps += s;
         if (vis <= 1e-4f) continue;
         out = out + albedo * V{L.emit[0], L.emit[1], L.emit[2]} * (ff * vis);
@@ -576,12 +687,13 @@ __device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V alb
         V to_light = c - p;
         float ff = sphere_light_ff(p, n, c, L.c[3]);
         if (ff <= 1e-6f) continue;
+        cnt.add(CN_LIGHT);
         float dist = len(to_light);
         float radius = fmaxf(L.c[3], 1e-4f);
         float k = clampr(dist / radius, 1.5f, 96.0f);
         float shadow_end = fmaxf(dist - radius * 1.25f, 0.05f);
         uint32_t s;
-        float vis = soft_shadow(sv, p + n * 3e-3f, to_light / dist, 0.015f, shadow_end, k, s);
+        float vis = soft_shadow(sv, p + n * 3e-3f, to_light / dist, 0.015f, shadow_end, k, s, cnt);
         steps += s;
         if (vis <= 1e-4f) continue;
         out = out + albedo * V{L.emit[0], L.emit[1], L.emit[2]} * (ff * vis);
@@ -657,7 +769,8 @@ struct GatherView {
 };
 
 // surfel.rs:262-293 with the cell walk of surfel.rs:127-140.
-__device__ __forceinline__ V gather(const GatherView& g, V p, V n) {
+template <class C>
+__device__ __forceinline__ V gather(const GatherView& g, V p, V n, C& cnt) {
     V acc{0.0f, 0.0f, 0.0f};
     float wsum = 0.0f;
     float r2 = g.radius * g.radius;
@@ -674,6 +787,7 @@ __device__ __forceinline__ V gather(const GatherView& g, V p, V n) {
             uint32_t e = __ldg(&g.starts[row + x1 + 1]);
             for (uint32_t k = s; k < e; ++k) {
                 float4 sp = __ldg(&g.gp[k]);
+                cnt.add(CN_GVISIT);
                 float d2 = dot(mk4(sp) - p, mk4(sp) - p);
                 if (d2 > r2) continue;
                 float4 sn = __ldg(&g.gn[k]);
@@ -681,6 +795,7 @@ __device__ __forceinline__ V gather(const GatherView& g, V p, V n) {
                 if (align <= 0.15f) continue;
                 float t = 1.0f - d2 / r2;
                 float w = t * t * align;
+                cnt.add(CN_GACCEPT);
                 float4 ir = __ldg(&g.girr[k]);
                 acc = acc + mk4(ir) * w;
                 wsum += w;

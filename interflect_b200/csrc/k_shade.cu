@@ -40,7 +40,9 @@ __device__ __forceinline__ GatherView gview(const GridParams& g) {
 }
 
 // main.rs:247-361 for one pixel.
-__device__ V shade_pixel(const SceneView& sv, const ShadeParams& P, uint32_t x, uint32_t y, uint32_t& evals) {
+template <class C>
+__device__ V shade_pixel(const SceneView& sv, const ShadeParams& P, uint32_t x, uint32_t y, uint32_t& evals,
+                         C& cnt) {
     const CamParams& c = P.cam;
     const V org{c.origin[0], c.origin[1], c.origin[2]};
     // main.rs:213-217
@@ -48,7 +50,7 @@ __device__ V shade_pixel(const SceneView& sv, const ShadeParams& P, uint32_t x, 
     float py = (1.0f - 2.0f * ((float)y + 0.5f) / (float)P.h) * c.tan_half;
     V rd = nrm(V{c.fwd[0], c.fwd[1], c.fwd[2]} + V{c.right[0], c.right[1], c.right[2]} * px +
                V{c.up[0], c.up[1], c.up[2]} * py);
-    TraceHit th = trace(sv, org, rd, 1e-3f, P.tmax);
+    TraceHit th = trace(sv, org, rd, 1e-3f, P.tmax, cnt);
     evals += th.steps;
     const bool tonemapped = P.mode <= 2;
     V e;
@@ -62,35 +64,35 @@ __device__ V shade_pixel(const SceneView& sv, const ShadeParams& P, uint32_t x, 
         float f = (float)th.steps / 128.0f;
         return V{f, 1.0f - f, 0.2f};
     }
-    const V n = scene_normal(sv, th.p);
+    const V n = scene_normal(sv, th.p, cnt);
     if (P.mode == 3) return n * 0.5f + V{0.5f, 0.5f, 0.5f};  // normals
     const DMaterial& m = sv.mats[th.mat];
     V col{0.0f, 0.0f, 0.0f};
     if (P.mode != 2) {
         uint32_t s = 0;
-        V d = direct(sv, th.p, n, -rd, m, s);
+        V d = direct(sv, th.p, n, -rd, m, s, cnt);
         evals += s;
         col = col + (d + V{m.emissive[0], m.emissive[1], m.emissive[2]});
     }
     if (P.has_gi) {
         GatherView g = gview(P.grid);
-        V irr = gather(g, th.p, n);
+        V irr = gather(g, th.p, n, cnt);
         col = col + V{m.kd[0], m.kd[1], m.kd[2]} * irr;
         if (m.f0[3] != 0.0f) {  // roughness < 0.45 || metallic > 0.05
             V refl = rd - n * (2.0f * dot(n, rd));
-            TraceHit rh = trace(sv, th.p + n * 1e-3f, refl, 1e-3f, P.tmax);
+            TraceHit rh = trace(sv, th.p + n * 1e-3f, refl, 1e-3f, P.tmax, cnt);
             evals += rh.steps;
             V rc;
             V e2;
             if (emitter_hit(sv, th.p, refl, fminf(rh.hit ? rh.t : kMaxF, P.tmax), e2)) {
                 rc = e2;
             } else if (rh.hit) {
-                const V n2 = scene_normal(sv, rh.p);
+                const V n2 = scene_normal(sv, rh.p, cnt);
                 const DMaterial& m2 = sv.mats[rh.mat];
                 uint32_t s2 = 0;
-                V d2 = direct(sv, rh.p, n2, -refl, m2, s2);
+                V d2 = direct(sv, rh.p, n2, -refl, m2, s2, cnt);
                 evals += s2;
-                V i2 = gather(g, rh.p, n2);
+                V i2 = gather(g, rh.p, n2, cnt);
                 rc = d2 + V{m2.kd[0], m2.kd[1], m2.kd[2]} * i2 + V{m2.emissive[0], m2.emissive[1], m2.emissive[2]};
             } else {
                 rc = sky();
@@ -104,8 +106,10 @@ __device__ V shade_pixel(const SceneView& sv, const ShadeParams& P, uint32_t x, 
     return col;
 }
 
+template <class C>
 __global__ void __launch_bounds__(128) k_shade(ShadeParams P) {
     IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
+    C cnt;
     __shared__ float t8[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) t8[i] = P.srgb_t[i];
     __syncthreads();
@@ -118,7 +122,7 @@ __global__ void __launch_bounds__(128) k_shade(ShadeParams P) {
         unsigned long long ev = 0;
         if (x < P.w && y < P.h) {
             uint32_t e = 0;
-            V c = shade_pixel(sv, P, x, y, e);
+            V c = shade_pixel(sv, P, x, y, e, cnt);
             ev = e;
             size_t o = ((size_t)y * P.w + x) * 3;
             if (P.film) {
@@ -137,15 +141,19 @@ __global__ void __launch_bounds__(128) k_shade(ShadeParams P) {
         for (int o = 16; o >= 1; o >>= 1) ev += __shfl_xor_sync(kFull, ev, o);
         if ((threadIdx.x & 31) == 0 && ev) atomicAdd(P.evals, ev);
     }
+    if constexpr (sizeof(C) > 1) cnt.flush(P.counts);
 }
 
 void launch_shade(cudaStream_t st, const ShadeParams& p) {
     unsigned long long tiles = (unsigned long long)((p.w + 15) / 16) * ((p.h + 7) / 8);
-    k_shade<<<grid_for(tiles * 128ull, 128, 16), 128, blob_smem(p.blob), st>>>(p);
+    const unsigned g = grid_for(tiles * 128ull, 128, 16);
+    if (p.counts) k_shade<Counts><<<g, 128, blob_smem(p.blob), st>>>(p);
+    else k_shade<NoCount><<<g, 128, blob_smem(p.blob), st>>>(p);
 }
 
 void configure_shade_kernels(int max_dyn_smem) {
-    cudaFuncSetAttribute(k_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_shade<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_shade<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }
 
 }  // namespace ifx

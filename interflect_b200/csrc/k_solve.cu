@@ -13,16 +13,19 @@ __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned lon
 }
 
 // solve.rs:27-39
+template <class C>
 __global__ void __launch_bounds__(128) k_light_surfels(BlobRef blob, SurfelArrays s, uint32_t n,
-                                                        unsigned long long* evals, uint32_t* status) {
+                                                        unsigned long long* evals, uint32_t* status,
+                                                        unsigned long long* counts) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
+    C cnt;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t limit = (n + stride - 1) / stride * stride;  // keep whole warps for the reduction
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < limit; i += stride) {
         unsigned long long e = 0;
         if (i < n) {
             uint32_t steps = 0;
-            V c = direct_diffuse(sv, mk4(s.p[i]), mk4(s.n[i]), mk4(s.albedo[i]), steps);
+            V c = direct_diffuse(sv, mk4(s.p[i]), mk4(s.n[i]), mk4(s.albedo[i]), steps, cnt);
             s.direct[i] = f4(c, 0.0f);
             s.rad[i] = f4(c, 0.0f);
             s.irr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -30,6 +33,7 @@ __global__ void __launch_bounds__(128) k_light_surfels(BlobRef blob, SurfelArray
         }
         block_add_u64(e, evals);
     }
+    if constexpr (sizeof(C) > 1) cnt.flush(counts);
 }
 
 // solve.rs:61-73: cluster radiosity as the area-weighted mean of its
@@ -84,8 +88,12 @@ __global__ void k_bounce_end(SolveCtl* ctl, uint32_t it) {
 }
 
 void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_t n, unsigned long long* evals,
-                          uint32_t* status) {
-    k_light_surfels<<<grid_for(n, 128, 16), 128, blob_smem(blob), st>>>(blob, s, n, evals, status);
+                          uint32_t* status, unsigned long long* counts) {
+    const unsigned g = grid_for(n, 128, 16);
+    if (counts)
+        k_light_surfels<Counts><<<g, 128, blob_smem(blob), st>>>(blob, s, n, evals, status, counts);
+    else
+        k_light_surfels<NoCount><<<g, 128, blob_smem(blob), st>>>(blob, s, n, evals, status, nullptr);
 }
 
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
@@ -99,7 +107,8 @@ void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const floa
 }
 
 void configure_solve_kernels(int max_dyn_smem) {
-    cudaFuncSetAttribute(k_light_surfels, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_light_surfels<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_light_surfels<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }
 
 }  // namespace ifx

@@ -11,6 +11,7 @@ namespace ifx {
 __global__ void __launch_bounds__(128) k_gen_project(BlobRef blob, SceneConsts sc, uint32_t seed0,
                                                       uint32_t count, float eps, float4* out, uint32_t* status) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
+    NoCount nc;
     const V lo{sc.lo[0], sc.lo[1], sc.lo[2]}, hi{sc.hi[0], sc.hi[1], sc.hi[2]};
     const float diag = sc.diag;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
@@ -19,15 +20,15 @@ __global__ void __launch_bounds__(128) k_gen_project(BlobRef blob, SceneConsts s
         V p = lo + (hi - lo) * s;
         bool ok = false;
         for (int it = 0; it < 10; ++it) {
-            float d = scene_dist(sv, p);
+            float d = scene_dist(sv, p, nc);
             if (fabsf(d) < eps) {
                 ok = true;
                 break;
             }
             if (!isfinite(d) || fabsf(d) > diag) break;
-            p = p - scene_normal(sv, p) * d;
+            p = p - scene_normal(sv, p, nc) * d;
         }
-        if (ok && fabsf(scene_dist(sv, p)) >= eps) ok = false;
+        if (ok && fabsf(scene_dist(sv, p, nc)) >= eps) ok = false;
         if (ok && (p.x < lo.x || p.y < lo.y || p.z < lo.z || p.x > hi.x || p.y > hi.y || p.z > hi.z)) ok = false;
         out[j] = make_float4(p.x, p.y, p.z, ok ? 1.0f : 0.0f);
     }
@@ -37,11 +38,12 @@ __global__ void __launch_bounds__(128) k_gen_project(BlobRef blob, SceneConsts s
 __global__ void __launch_bounds__(128) k_gen_finalize(BlobRef blob, const float4* pts, uint32_t n, float area,
                                                        SurfelArrays s, uint32_t* status) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
+    NoCount nc;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         V p = mk4(pts[i]);
-        DistHit h = dist_mat(sv, p);
+        DistHit h = dist_mat(sv, p, nc);
         const DMaterial& m = sv.mats[h.mat];
-        V nn = scene_normal(sv, p);
+        V nn = scene_normal(sv, p, nc);
         s.p[i] = f4(p, area);
         s.n[i] = f4(nn, 0.0f);
         s.albedo[i] = make_float4(m.kd[0], m.kd[1], m.kd[2], 0.0f);

@@ -71,12 +71,15 @@ __global__ void __launch_bounds__(256) k_pair_fill(const float4* sp, const float
 }
 
 // formfactor.rs:194-205: the visibility cone of one candidate pair.
+template <class C>
 __global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc, const float4* sp,
                                                      const float4* sn, const float4* cp, const float4* cn,
                                                      const uint32_t* cand_c, const uint32_t* cand_row,
                                                      unsigned long long ncand, float* cand_vis,
-                                                     uint8_t* cand_steps, uint32_t* status) {
+                                                     uint8_t* cand_steps, uint32_t* status,
+                                                     unsigned long long* counts) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
+    C cnt;
     const float off = sc.diag * 5e-4f, tmin = sc.diag * 1e-3f;
     for (unsigned long long j = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j < ncand;
          j += (unsigned long long)gridDim.x * blockDim.x) {
@@ -88,20 +91,24 @@ __global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc
         V dir = d / r;
         float k = clampr(r / fmaxf(cnc.w, 1e-4f), 1.5f, 32.0f);
         uint32_t steps;
-        float vis = soft_shadow(sv, p + nn * off, dir, tmin, r - cnc.w * 0.75f, k, steps);
+        float vis = soft_shadow(sv, p + nn * off, dir, tmin, r - cnc.w * 0.75f, k, steps, cnt);
         cand_vis[j] = vis;
         cand_steps[j] = (uint8_t)steps;
     }
+    if constexpr (sizeof(C) > 1) cnt.flush(counts);
 }
 
 // trace.rs:165-186: 16 lanes per row (one ray each); lane 0 of the 16
 // writes the row's open-ray count and the rays' SDF evaluations. A hit's
 // normal is never used here, so it is not computed, but its four taps are
 // still counted (trace.rs:48).
+template <class C>
 __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, const float4* sp,
                                                   const float4* sn, uint32_t n, uint32_t* row_open,
-                                                  uint32_t* row_csteps, uint32_t* status) {
+                                                  uint32_t* row_csteps, uint32_t* status,
+                                                  unsigned long long* counts) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
+    C cnt;
     const int lane = threadIdx.x & 31;
     const unsigned long long total = (unsigned long long)n * 16ull;
     const unsigned long long padded = (total + 31ull) & ~31ull;
@@ -116,7 +123,7 @@ __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, c
             V t, b;
             frame(nn, t, b);
             V d = t * sc.closure[k][0] + b * sc.closure[k][1] + nn * sc.closure[k][2];
-            TraceHit h = trace(sv, p + nn * 1e-3f, nrm(d), 1e-3f, tmax);
+            TraceHit h = trace(sv, p + nn * 1e-3f, nrm(d), 1e-3f, tmax, cnt);
             open = h.hit ? 0u : 1u;
             steps = h.steps;
         }
@@ -128,6 +135,7 @@ __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, c
             row_csteps[row] = steps;
         }
     }
+    if constexpr (sizeof(C) > 1) cnt.flush(counts);
 }
 
 // formfactor.rs:206-238: links are pairs with vis > 1e-3, weighted ff*vis,
@@ -254,15 +262,26 @@ void launch_pair_fill(cudaStream_t st, const float4* sp, const float4* sn, uint3
 }
 void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
                        const float4* cp, const float4* cn, const uint32_t* cand_c, const uint32_t* cand_row,
-                       unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status) {
+                       unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status,
+                       unsigned long long* counts) {
     if (ncand == 0) return;
-    k_visibility<<<grid_for(ncand, 128, 16), 128, blob_smem(blob), st>>>(blob, sc, sp, sn, cp, cn, cand_c, cand_row,
-                                                                        ncand, cand_vis, cand_steps, status);
+    const unsigned g = grid_for(ncand, 128, 16);
+    if (counts)
+        k_visibility<Counts><<<g, 128, blob_smem(blob), st>>>(blob, sc, sp, sn, cp, cn, cand_c, cand_row, ncand,
+                                                              cand_vis, cand_steps, status, counts);
+    else
+        k_visibility<NoCount><<<g, 128, blob_smem(blob), st>>>(blob, sc, sp, sn, cp, cn, cand_c, cand_row, ncand,
+                                                               cand_vis, cand_steps, status, nullptr);
 }
 void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
-                    uint32_t n, uint32_t* row_open, uint32_t* row_csteps, uint32_t* status) {
-    k_closure<<<grid_for((unsigned long long)n * 16ull, 128, 16), 128, blob_smem(blob), st>>>(
-        blob, sc, sp, sn, n, row_open, row_csteps, status);
+                    uint32_t n, uint32_t* row_open, uint32_t* row_csteps, uint32_t* status,
+                    unsigned long long* counts) {
+    const unsigned g = grid_for((unsigned long long)n * 16ull, 128, 16);
+    if (counts)
+        k_closure<Counts><<<g, 128, blob_smem(blob), st>>>(blob, sc, sp, sn, n, row_open, row_csteps, status, counts);
+    else
+        k_closure<NoCount><<<g, 128, blob_smem(blob), st>>>(blob, sc, sp, sn, n, row_open, row_csteps, status,
+                                                            nullptr);
 }
 void launch_row_finalize(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const float* cand_ff,
                          const float* cand_vis, const uint8_t* cand_steps, const uint32_t* row_open,
@@ -287,8 +306,10 @@ void launch_sum_u64(cudaStream_t st, const unsigned long long* v, uint32_t n, un
 }
 
 void configure_transfer_kernels(int max_dyn_smem) {
-    cudaFuncSetAttribute(k_visibility, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
-    cudaFuncSetAttribute(k_closure, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_visibility<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_visibility<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_closure<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_closure<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }
 
 }  // namespace ifx

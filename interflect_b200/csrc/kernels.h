@@ -71,9 +71,11 @@ void launch_pair_fill(cudaStream_t st, const float4* sp, const float4* sn, uint3
                       float* cand_ff, uint32_t* cand_row);
 void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
                        const float4* cp, const float4* cn, const uint32_t* cand_c, const uint32_t* cand_row,
-                       unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status);
+                       unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status,
+                       unsigned long long* counts = nullptr);
 void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
-                    uint32_t n, uint32_t* row_open, uint32_t* row_csteps, uint32_t* status);
+                    uint32_t n, uint32_t* row_open, uint32_t* row_csteps, uint32_t* status,
+                    unsigned long long* counts = nullptr);
 void launch_row_finalize(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const float* cand_ff,
                          const float* cand_vis, const uint8_t* cand_steps, const uint32_t* row_open,
                          const uint32_t* row_csteps, uint32_t* row_links, float* row_scale, float* row_sum,
@@ -95,7 +97,7 @@ struct SolveCtl {
     uint32_t last_residual;  // residual of the last completed bounce
 };
 void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_t n, unsigned long long* evals,
-                          uint32_t* status);
+                          uint32_t* status, unsigned long long* counts = nullptr);
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
                          const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches);
@@ -122,6 +124,7 @@ struct ShadeParams {
     uint8_t* out8;        // w*h*3, nullable
     unsigned long long* evals;
     uint32_t* status;
+    unsigned long long* counts;  // non-null: the counting instantiation (work counters, kNumCounters u64)
 };
 void launch_shade(cudaStream_t st, const ShadeParams& p);
 
