@@ -63,7 +63,11 @@ struct ifx_ctx {
     bool has_transfer = false;
     uint64_t ncand = 0, links = 0;
     DBuf cand_count, cand_off, cand_c, cand_ff, cand_row, cand_vis, cand_steps;
-    DBuf row_open, row_csteps, row_links, row_scale, row_sum, row_sky, row_evals, starts, idx, w;
+    DBuf clo, row_links, row_scale, row_sum, row_sky, row_evals, starts, idx, w;
+    DBuf qcur;  // persistent-kernel cursors (16 x u64), zeroed before each use
+
+    // shade wavefront
+    DBuf hp1, hn1, hp2, hn2, ff1, vis1, ff2, vis2, q1, q2, qr, qlen;
 
     // solve
     DBuf cluster_rad, ctl;
@@ -293,6 +297,8 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
     if (ensure(ctx, ctx->work, 4 * IFX_WORK_COUNTERS * 8) != IFX_OK ||
         cudaMemsetAsync(ctx->work.p, 0, 4 * IFX_WORK_COUNTERS * 8, ctx->st) != cudaSuccess)
         return bail(cudaErrorMemoryAllocation);
+    if (ensure(ctx, ctx->qcur, 16 * 8) != IFX_OK || ensure(ctx, ctx->qlen, 16) != IFX_OK)
+        return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->status, 16) != IFX_OK || ensure(ctx, ctx->small, 64) != IFX_OK ||
         ensure(ctx, ctx->srgb_t, 256 * sizeof(float)) != IFX_OK || ensure(ctx, ctx->ctl, sizeof(SolveCtl)) != IFX_OK)
         return bail(cudaErrorMemoryAllocation);
@@ -315,7 +321,9 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->srad, &ctx->keys, &ctx->keys_alt, &ctx->heads, &ctx->head_scan, &ctx->seg_start,
                     &ctx->members, &ctx->cp_tmp, &ctx->cn_tmp, &ctx->valid, &ctx->valid_scan, &ctx->cp, &ctx->cn,
                     &ctx->crange, &ctx->cand_count, &ctx->cand_off, &ctx->cand_c, &ctx->cand_ff, &ctx->cand_row,
-                    &ctx->cand_vis, &ctx->cand_steps, &ctx->row_open, &ctx->row_csteps, &ctx->row_links,
+                    &ctx->cand_vis, &ctx->cand_steps, &ctx->clo, &ctx->qcur, &ctx->hp1, &ctx->hn1, &ctx->hp2,
+                    &ctx->hn2, &ctx->ff1, &ctx->vis1, &ctx->ff2, &ctx->vis2, &ctx->q1, &ctx->q2, &ctx->qr,
+                    &ctx->qlen, &ctx->row_links,
                     &ctx->row_scale, &ctx->row_sum, &ctx->row_sky, &ctx->row_evals, &ctx->starts, &ctx->idx,
                     &ctx->w, &ctx->cluster_rad, &ctx->ctl, &ctx->gkeys, &ctx->gkeys_alt, &ctx->gstarts, &ctx->gp,
                     &ctx->gn, &ctx->girr, &ctx->gitems, &ctx->film, &ctx->out8, &ctx->cub_tmp, &ctx->small,
@@ -383,12 +391,13 @@ extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     if (!ctx || !scene) return fail(ctx, IFX_ERR_INVALID, "null argument");
     CK(cudaSetDevice(ctx->device));
     const HScene& s = scene->s;
-    // The device traversal stack holds 64 entries, as the reference's does;
-    // reject a tree that could overflow it (never reached by SAH trees of
-    // scenes within the parser's limits).
+    // Size each thread's traversal stack to the tree: a near-first DFS holds
+    // at most depth + 1 entries. The reference's stack has 64 entries, so a
+    // deeper tree is rejected (never reached by SAH trees within the
+    // parser's limits).
+    int maxd = 0;
     {
         std::vector<int> depth(s.nodes.size(), 0);
-        int maxd = 0;
         for (size_t i = 0; i < s.nodes.size(); ++i) {
             maxd = std::max(maxd, depth[i]);
             if (s.nodes[i].count == 0) {
@@ -406,6 +415,7 @@ extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     ctx->blobref.ptr = (const uint8_t*)ctx->blob.p;
     ctx->blobref.bytes = (uint32_t)blob.size();
     ctx->blobref.staged = blob.size() <= kMaxStagedBlob ? 1 : 0;
+    ctx->blobref.stack_depth = maxd + 2;
     ctx->sc = scene_consts(s);
     ctx->has_scene = true;
     ctx->has_transfer = false;
@@ -688,6 +698,7 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     unsigned long long ncand = 0;
     CK(cudaMemcpyAsync(&ncand, (unsigned long long*)ctx->cand_off.p + n, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    if (ncand >= 0xffffffffull) return fail(ctx, IFX_ERR_LIMIT, "more than 2^32 - 1 candidate pairs");
     ENSURE(ctx->cand_c, ncand * 4);
     ENSURE(ctx->cand_ff, ncand * 4);
     ENSURE(ctx->cand_row, ncand * 4);
@@ -698,19 +709,20 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     ctx->launches++;
     CKL();
 
-    // Visibility and closure.
-    ENSURE(ctx->row_open, (size_t)n * 4);
-    ENSURE(ctx->row_csteps, (size_t)n * 4);
+    // Visibility and closure (persistent kernels; cursors start at zero).
+    ENSURE(ctx->clo, (size_t)n * 16 * 2);
+    unsigned long long* cur = (unsigned long long*)ctx->qcur.p;
+    CK(cudaMemsetAsync(cur, 0, 16 * 8, ctx->st));
     CK(cudaEventRecord(ctx->kv0, ctx->st));
     launch_visibility(ctx->st, ctx->blobref, ctx->sc, sp, sn, cp, cn, (const uint32_t*)ctx->cand_c.p,
                       (const uint32_t*)ctx->cand_row.p, ncand, (float*)ctx->cand_vis.p,
-                      (uint8_t*)ctx->cand_steps.p, status, ctx->work_of(IFX_KERNEL_VISIBILITY));
+                      (uint8_t*)ctx->cand_steps.p, status, ctx->work_of(IFX_KERNEL_VISIBILITY), &cur[0]);
     if (ncand) ctx->launches++;
     CKL();
     CK(cudaEventRecord(ctx->kv1, ctx->st));
     CK(cudaEventRecord(ctx->kc0, ctx->st));
-    launch_closure(ctx->st, ctx->blobref, ctx->sc, sp, sn, n, (uint32_t*)ctx->row_open.p,
-                   (uint32_t*)ctx->row_csteps.p, status, ctx->work_of(IFX_KERNEL_CLOSURE));
+    launch_closure(ctx->st, ctx->blobref, ctx->sc, sp, sn, n, (uint16_t*)ctx->clo.p, status,
+                   ctx->work_of(IFX_KERNEL_CLOSURE), &cur[1]);
     ctx->launches++;
     CKL();
     CK(cudaEventRecord(ctx->kc1, ctx->st));
@@ -724,8 +736,8 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     ENSURE(ctx->starts, ((size_t)n + 1) * 4);
     launch_row_finalize(ctx->st, n, (const unsigned long long*)ctx->cand_off.p, (const float*)ctx->cand_ff.p,
                         (const float*)ctx->cand_vis.p, (const uint8_t*)ctx->cand_steps.p,
-                        (const uint32_t*)ctx->row_open.p, (const uint32_t*)ctx->row_csteps.p,
-                        (uint32_t*)ctx->row_links.p, (float*)ctx->row_scale.p, (float*)ctx->row_sum.p,
+                        (const uint16_t*)ctx->clo.p, (uint32_t*)ctx->row_links.p, (float*)ctx->row_scale.p,
+                        (float*)ctx->row_sum.p,
                         (float*)ctx->row_sky.p, (unsigned long long*)ctx->row_evals.p);
     ctx->launches++;
     CKL();
@@ -1033,10 +1045,39 @@ extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, u
     P.evals = &small[3];
     P.status = (uint32_t*)ctx->status.p;
     P.counts = ctx->work_of(IFX_KERNEL_SHADE);
+    // Wavefront buffers (grow-only).
+    const int nl = (int)(s.lights.size() + s.sphere_lights.size());
+    const size_t slots = px * (size_t)(nl > 0 ? nl : 1);
+    ENSURE(ctx->hp1, px * 16);
+    ENSURE(ctx->hn1, px * 16);
+    ENSURE(ctx->hp2, px * 16);
+    ENSURE(ctx->hn2, px * 16);
+    ENSURE(ctx->ff1, slots * 4);
+    ENSURE(ctx->vis1, slots * 4);
+    ENSURE(ctx->ff2, slots * 4);
+    ENSURE(ctx->vis2, slots * 4);
+    ENSURE(ctx->q1, slots * 4);
+    ENSURE(ctx->q2, slots * 4);
+    ENSURE(ctx->qr, px * 4);
+    P.hp1 = (float4*)ctx->hp1.p;
+    P.hn1 = (float4*)ctx->hn1.p;
+    P.hp2 = (float4*)ctx->hp2.p;
+    P.hn2 = (float4*)ctx->hn2.p;
+    P.ff1 = (float*)ctx->ff1.p;
+    P.vis1 = (float*)ctx->vis1.p;
+    P.ff2 = (float*)ctx->ff2.p;
+    P.vis2 = (float*)ctx->vis2.p;
+    P.q1 = (uint32_t*)ctx->q1.p;
+    P.q2 = (uint32_t*)ctx->q2.p;
+    P.qr = (uint32_t*)ctx->qr.p;
+    P.qlen = (uint32_t*)ctx->qlen.p;
+    P.cursors = (unsigned long long*)ctx->qcur.p;
+    P.nl = nl;
     CK(cudaMemsetAsync(&small[3], 0, 8, ctx->st));
+    CK(cudaMemsetAsync(ctx->qlen.p, 0, 16, ctx->st));
+    CK(cudaMemsetAsync(ctx->qcur.p, 0, 16 * 8, ctx->st));
     CK(cudaEventRecord(ctx->ev0, ctx->st));
-    launch_shade(ctx->st, P);
-    ctx->launches++;
+    ctx->launches += (uint64_t)launch_shade(ctx->st, P);
     CKL();
     CK(cudaEventRecord(ctx->ev1, ctx->st));
     unsigned long long e = 0;

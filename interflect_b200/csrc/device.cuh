@@ -64,11 +64,19 @@ struct SceneView {
     const DMaterial* mats;
     const uint32_t* linear;
     int n_planes, n_objects, n_nodes, n_lights, n_slights, use_bvh;
+    // This thread's BVH traversal stack in shared memory: entry i lives at
+    // stk[i * stk_stride]; stk_depth entries (the tree depth + 2, fixed by
+    // the host), so consecutive threads hit consecutive banks.
+    uint32_t* stk;
+    int stk_stride, stk_depth;
 };
 
 __device__ __forceinline__ SceneView make_view(const uint8_t* base) {
     const BlobHeader* h = reinterpret_cast<const BlobHeader*>(base);
     SceneView v;
+    v.stk = nullptr;
+    v.stk_stride = 0;
+    v.stk_depth = 0;
     v.objs = reinterpret_cast<const DObject*>(base + h->off_objects);
     v.prims = reinterpret_cast<const DPrim*>(base + h->off_prims);
     v.nodes = reinterpret_cast<const DNode*>(base + h->off_nodes);
@@ -295,11 +303,14 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
     }
     if (sv.use_bvh) {
         if (sv.n_nodes == 0) return best;
-        int stack[64];
+        uint32_t* const stack = sv.stk;
+        const int stride = sv.stk_stride;
         int sp = 0;
-        stack[sp++] = 0;
+        stack[0] = 0;
+        sp = 1;
         while (sp > 0) {
-            const int ni = stack[--sp];
+            --sp;
+            const int ni = (int)stack[sp * stride];
             const DNode nd = sv.nodes[ni];
             if (aabb_dist(p, nd, cnt) >= best.d) continue;
             if (nd.count > 0) {
@@ -315,16 +326,19 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
                 const int l = ni + 1, r = nd.link;
                 float dl = aabb_dist(p, sv.nodes[l], cnt);
                 float dr = aabb_dist(p, sv.nodes[r], cnt);
-                // The stack holds 64 entries like the reference's; a BVH
-                // needs depth + 1, far below that for any scene the parser
-                // accepts (the host rejects deeper trees).
+                // Near-first DFS holds at most depth + 1 entries; the host
+                // sizes the stack to depth + 2 (and rejects trees deeper
+                // than the reference's 64-entry stack). The guard keeps an
+                // unexpected overflow inside the stack: traversal stops.
+                if (sp + 2 > sv.stk_depth) break;
                 if (dl < dr) {
-                    stack[sp++] = r;
-                    stack[sp++] = l;
+                    stack[sp * stride] = (uint32_t)r;
+                    stack[(sp + 1) * stride] = (uint32_t)l;
                 } else {
-                    stack[sp++] = l;
-                    stack[sp++] = r;
+                    stack[sp * stride] = (uint32_t)l;
+                    stack[(sp + 1) * stride] = (uint32_t)r;
                 }
+                sp += 2;
             }
         }
     } else {
@@ -423,6 +437,95 @@ __device__ __forceinline__ float soft_shadow(const SceneView& sv, V ro, V rd, fl
     }
     steps_out = steps;
     return clampr(res, 0.0f, 1.0f);
+}
+
+// ------------------------------------------------- resumable ray marches ----
+// The loops of trace() and soft_shadow() split into single steps, so that a
+// persistent kernel can advance many rays one SDF query at a time and refill
+// lanes whose ray ended. The arithmetic per step is exactly the loop body's.
+
+// trace.rs:84-124 as a state machine.
+struct ShadowRay {
+    V ro, rd;
+    float t, tmax, k, res, ph;
+    uint32_t steps;
+};
+__device__ __forceinline__ ShadowRay shadow_begin(V ro, V rd, float tmin, float tmax, float k) {
+    return ShadowRay{ro, rd, tmin, tmax, k, 1.0f, 1e20f, 0u};
+}
+// True when the march cannot take a first step (the loop body never runs).
+__device__ __forceinline__ bool shadow_done_before_start(const ShadowRay& s) { return !(s.t < s.tmax); }
+// One loop iteration. Returns true when the march has ended, with `vis` set.
+template <class C>
+__device__ __forceinline__ bool shadow_step(const SceneView& sv, ShadowRay& s, float& vis, C& cnt) {
+    float h = scene_dist(sv, s.ro + s.rd * s.t, cnt);
+    cnt.add(CN_SSTEP);
+    s.steps += 1;
+    if (h < 1e-4f) {
+        vis = 0.0f;
+        return true;
+    }
+    float y, d;
+    if (h < s.ph) {
+        y = h * h / (2.0f * s.ph);
+        d = sqrtf(fmaxf(h * h - y * y, 0.0f));
+    } else {
+        y = 0.0f;
+        d = h;
+    }
+    s.res = fminf(s.res, s.k * d / fmaxf(s.t - y, 1e-4f));
+    if (s.res < 1e-3f) {
+        vis = 0.0f;
+        return true;
+    }
+    s.ph = h;
+    s.t += clampr(h, 0.006f, 0.12f);
+    if (!(s.steps < kShadowSteps && s.t < s.tmax)) {
+        vis = clampr(s.res, 0.0f, 1.0f);
+        return true;
+    }
+    return false;
+}
+
+// trace.rs:27-58 as a state machine.
+struct TraceRay {
+    V ro, rd;
+    float t, tmax;
+    uint32_t steps;
+};
+enum : int { kMarching = 0, kHit = 1, kMiss = 2 };
+// One loop iteration. On kHit, `p`/`mat` are the hit and r.t its distance;
+// r.steps then includes the four normal taps (trace.rs:48).
+template <class C>
+__device__ __forceinline__ int trace_step(const SceneView& sv, TraceRay& r, V& p, uint32_t& mat, C& cnt) {
+    p = r.ro + r.rd * r.t;
+    DistHit h = dist_mat(sv, p, cnt);
+    cnt.add(CN_TSTEP);
+    r.steps += 1;
+    float eps = 1e-4f * fmaxf(r.t, 1.0f);
+    if (h.d < eps) {
+        mat = h.mat;
+        r.steps += 4;
+        return kHit;
+    }
+    r.t += h.d;
+    if (r.t > r.tmax || r.steps >= kMaxSteps) return kMiss;
+    return kMarching;
+}
+
+// scene.rs:218-236 with the four taps in a rolled loop (one query site).
+template <class C>
+__device__ __forceinline__ V scene_normal_rolled(const SceneView& sv, V p, C& cnt) {
+    const float H = 5e-4f;
+    V n{0.0f, 0.0f, 0.0f};
+#pragma unroll 1
+    for (int i = 0; i < 4; ++i) {
+        V k{(i == 0 || i == 3) ? 1.0f : -1.0f, (i >= 2) ? 1.0f : -1.0f, (i == 1 || i == 3) ? 1.0f : -1.0f};
+        n = n + k * scene_dist(sv, p + k * H, cnt);
+    }
+    float l = len(n);
+    if (l > 1e-12f) return n / l;
+    return V{0.0f, 1.0f, 0.0f};
 }
 
 // ltc.rs:88-96

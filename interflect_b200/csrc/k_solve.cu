@@ -37,19 +37,48 @@ __global__ void __launch_bounds__(128) k_light_surfels(BlobRef blob, SurfelArray
 }
 
 // solve.rs:61-73: cluster radiosity as the area-weighted mean of its
-// members' radiosity, summed sequentially in member order.
-__global__ void __launch_bounds__(128) k_cluster_agg(const float4* rad, const float4* sp, const float4* cp,
-                                                      const uint2* crange, const uint32_t* members, uint32_t nc,
-                                                      float4* cluster_rad, const SolveCtl* ctl) {
+// members' radiosity, summed sequentially in member order. One CTA per
+// cluster: the threads gather members' rad * area (each product exact per
+// element) into shared memory chunk by chunk, double-buffered, and thread 0
+// adds them in member order.
+static constexpr int kAggBlock = 128;
+__global__ void __launch_bounds__(kAggBlock) k_cluster_agg(const float4* rad, const float4* sp, const float4* cp,
+                                                            const uint2* crange, const uint32_t* members,
+                                                            uint32_t nc, float4* cluster_rad, const SolveCtl* ctl) {
     if (ctl->done) return;
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-        uint2 r = crange[c];
+    __shared__ float4 buf[2][kAggBlock];
+    for (uint32_t c = blockIdx.x; c < nc; c += gridDim.x) {
+        const uint2 r = crange[c];
+        const uint32_t len = r.y - r.x;
+        const uint32_t chunks = (len + kAggBlock - 1) / kAggBlock;
+        auto load = [&](uint32_t ch, int b) {
+            uint32_t k = r.x + ch * kAggBlock + threadIdx.x;
+            if (k < r.y) {
+                uint32_t m = __ldg(&members[k]);
+                float4 v = rad[m];
+                float a = __ldg(&sp[m].w);
+                buf[b][threadIdx.x] = make_float4(v.x * a, v.y * a, v.z * a, 0.0f);
+            }
+        };
+        if (chunks) load(0, 0);
+        __syncthreads();
         V acc{0.0f, 0.0f, 0.0f};
-        for (uint32_t k = r.x; k < r.y; ++k) {
-            uint32_t m = __ldg(&members[k]);
-            acc = acc + mk4(rad[m]) * __ldg(&sp[m].w);
+        for (uint32_t ch = 0; ch < chunks; ++ch) {
+            const int b = ch & 1;
+            if (threadIdx.x == 0) {
+                const uint32_t cnt = min((uint32_t)kAggBlock, len - ch * kAggBlock);
+                for (uint32_t k = 0; k < cnt; ++k) {
+                    float4 v = buf[b][k];
+                    acc = acc + V{v.x, v.y, v.z};
+                }
+                if (ch + 1 < chunks) load(ch + 1, b ^ 1);
+            } else if (ch + 1 < chunks) {
+                load(ch + 1, b ^ 1);
+            }
+            __syncthreads();
         }
-        cluster_rad[c] = f4(acc / fmaxf(cp[c].w, 1e-12f), 0.0f);
+        if (threadIdx.x == 0) cluster_rad[c] = f4(acc / fmaxf(cp[c].w, 1e-12f), 0.0f);
+        __syncthreads();
     }
 }
 
@@ -91,15 +120,16 @@ void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_
                           uint32_t* status, unsigned long long* counts) {
     const unsigned g = grid_for(n, 128, 16);
     if (counts)
-        k_light_surfels<Counts><<<g, 128, blob_smem(blob), st>>>(blob, s, n, evals, status, counts);
+        k_light_surfels<Counts><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, counts);
     else
-        k_light_surfels<NoCount><<<g, 128, blob_smem(blob), st>>>(blob, s, n, evals, status, nullptr);
+        k_light_surfels<NoCount><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, nullptr);
 }
 
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
                          const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches) {
-    k_cluster_agg<<<grid_for(nc, 128), 128, 0, st>>>(s.rad, s.p, cp, crange, members, nc, cluster_rad, ctl);
+    k_cluster_agg<<<nc < 4096u ? nc : 4096u, kAggBlock, 0, st>>>(s.rad, s.p, cp, crange, members, nc, cluster_rad,
+                                                                   ctl);
     k_jacobi<<<grid_for(n, 256), 256, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, starts, idx, w, cluster_rad,
                                                ctl);
     k_bounce_end<<<1, 1, 0, st>>>(ctl, it);

@@ -55,11 +55,11 @@ __global__ void __launch_bounds__(128) k_gen_finalize(BlobRef blob, const float4
 
 void launch_gen_project(cudaStream_t st, BlobRef blob, SceneConsts sc, uint32_t seed0, uint32_t count, float eps,
                         float4* out, uint32_t* status) {
-    k_gen_project<<<grid_for(count, 128), 128, blob_smem(blob), st>>>(blob, sc, seed0, count, eps, out, status);
+    k_gen_project<<<grid_for(count, 128), 128, blob_smem(blob, 128), st>>>(blob, sc, seed0, count, eps, out, status);
 }
 void launch_gen_finalize(cudaStream_t st, BlobRef blob, const float4* pts, uint32_t n, float area, SurfelArrays s,
                          uint32_t* status) {
-    k_gen_finalize<<<grid_for(n, 128), 128, blob_smem(blob), st>>>(blob, pts, n, area, s, status);
+    k_gen_finalize<<<grid_for(n, 128), 128, blob_smem(blob, 128), st>>>(blob, pts, n, area, s, status);
 }
 
 // ------------------------------------------------------------ clusters ----

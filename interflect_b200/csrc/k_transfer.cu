@@ -71,68 +71,95 @@ __global__ void __launch_bounds__(256) k_pair_fill(const float4* sp, const float
 }
 
 // formfactor.rs:194-205: the visibility cone of one candidate pair.
+// Persistent: each lane marches one candidate's cone one SDF query per
+// iteration and takes a new candidate from its warp's queue when the cone
+// ends, so a warp stays full however uneven the cones' lengths are.
 template <class C>
 __global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc, const float4* sp,
                                                      const float4* sn, const float4* cp, const float4* cn,
                                                      const uint32_t* cand_c, const uint32_t* cand_row,
                                                      unsigned long long ncand, float* cand_vis,
                                                      uint8_t* cand_steps, uint32_t* status,
-                                                     unsigned long long* counts) {
+                                                     unsigned long long* counts, unsigned long long* cursor) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
     C cnt;
+    WarpQueue q;
     const float off = sc.diag * 5e-4f, tmin = sc.diag * 1e-3f;
-    for (unsigned long long j = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j < ncand;
-         j += (unsigned long long)gridDim.x * blockDim.x) {
-        const uint32_t row = cand_row[j], c = cand_c[j];
-        const V p = mk4(__ldg(&sp[row])), nn = mk4(__ldg(&sn[row]));
-        const float4 cpc = __ldg(&cp[c]), cnc = __ldg(&cn[c]);
-        V d = mk4(cpc) - p;
-        float r = sqrtf(dot(d, d));
-        V dir = d / r;
-        float k = clampr(r / fmaxf(cnc.w, 1e-4f), 1.5f, 32.0f);
-        uint32_t steps;
-        float vis = soft_shadow(sv, p + nn * off, dir, tmin, r - cnc.w * 0.75f, k, steps, cnt);
-        cand_vis[j] = vis;
-        cand_steps[j] = (uint8_t)steps;
+    uint32_t item = ~0u;
+    ShadowRay ray;
+    while (true) {
+        const uint32_t got = q.refill(item == ~0u, ncand, cursor);
+        if (got != ~0u) {
+            const uint32_t row = cand_row[got], c = cand_c[got];
+            const V p = mk4(__ldg(&sp[row])), nn = mk4(__ldg(&sn[row]));
+            const float4 cpc = __ldg(&cp[c]), cnc = __ldg(&cn[c]);
+            V d = mk4(cpc) - p;
+            float r = sqrtf(dot(d, d));
+            V dir = d / r;
+            float k = clampr(r / fmaxf(cnc.w, 1e-4f), 1.5f, 32.0f);
+            ray = shadow_begin(p + nn * off, dir, tmin, r - cnc.w * 0.75f, k);
+            if (shadow_done_before_start(ray)) {
+                cand_vis[got] = clampr(ray.res, 0.0f, 1.0f);
+                cand_steps[got] = 0;
+            } else {
+                item = got;
+            }
+        }
+        if (!__any_sync(kFull, item != ~0u)) {
+            if (q.empty()) break;
+            continue;
+        }
+        if (item != ~0u) {
+            float vis;
+            if (shadow_step(sv, ray, vis, cnt)) {
+                cand_vis[item] = vis;
+                cand_steps[item] = (uint8_t)ray.steps;
+                item = ~0u;
+            }
+        }
     }
     if constexpr (sizeof(C) > 1) cnt.flush(counts);
 }
 
-// trace.rs:165-186: 16 lanes per row (one ray each); lane 0 of the 16
-// writes the row's open-ray count and the rays' SDF evaluations. A hit's
-// normal is never used here, so it is not computed, but its four taps are
-// still counted (trace.rs:48).
+// trace.rs:165-186: one persistent lane per hemisphere ray (16 per row);
+// each ray's result is written to its own slot as (open << 8) | steps and
+// k_row_finalize reduces the row's 16 slots. A hit's normal is never used
+// here, so it is not computed, but its four taps are still counted
+// (trace.rs:48).
 template <class C>
 __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, const float4* sp,
-                                                  const float4* sn, uint32_t n, uint32_t* row_open,
-                                                  uint32_t* row_csteps, uint32_t* status,
-                                                  unsigned long long* counts) {
+                                                  const float4* sn, uint32_t n, uint16_t* clo, uint32_t* status,
+                                                  unsigned long long* counts, unsigned long long* cursor) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
     C cnt;
-    const int lane = threadIdx.x & 31;
+    WarpQueue q;
     const unsigned long long total = (unsigned long long)n * 16ull;
-    const unsigned long long padded = (total + 31ull) & ~31ull;
     const float tmax = sc.diag * 2.0f;
-    for (unsigned long long g = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; g < padded;
-         g += (unsigned long long)gridDim.x * blockDim.x) {
-        const bool valid = g < total;
-        uint32_t open = 0, steps = 0;
-        if (valid) {
-            const uint32_t row = (uint32_t)(g >> 4), k = (uint32_t)(g & 15ull);
+    uint32_t item = ~0u;
+    TraceRay ray;
+    while (true) {
+        const uint32_t got = q.refill(item == ~0u, total, cursor);
+        if (got != ~0u) {
+            const uint32_t row = got >> 4, k = got & 15u;
             const V p = mk4(__ldg(&sp[row])), nn = mk4(__ldg(&sn[row]));
             V t, b;
             frame(nn, t, b);
             V d = t * sc.closure[k][0] + b * sc.closure[k][1] + nn * sc.closure[k][2];
-            TraceHit h = trace(sv, p + nn * 1e-3f, nrm(d), 1e-3f, tmax, cnt);
-            open = h.hit ? 0u : 1u;
-            steps = h.steps;
+            ray = TraceRay{p + nn * 1e-3f, nrm(d), 1e-3f, tmax, 0u};
+            item = got;
         }
-        unsigned om = __ballot_sync(kFull, open != 0);
-        for (int o = 8; o >= 1; o >>= 1) steps += __shfl_xor_sync(kFull, steps, o);
-        if (valid && (lane & 15) == 0) {
-            const uint32_t row = (uint32_t)(g >> 4);
-            row_open[row] = __popc(om & (0xffffu << (lane & 16)));
-            row_csteps[row] = steps;
+        if (!__any_sync(kFull, item != ~0u)) {
+            if (q.empty()) break;
+            continue;
+        }
+        if (item != ~0u) {
+            V hp;
+            uint32_t hm;
+            const int st = trace_step(sv, ray, hp, hm, cnt);
+            if (st != kMarching) {
+                clo[item] = (uint16_t)(((st == kMiss) ? 0x100u : 0u) | ray.steps);
+                item = ~0u;
+            }
         }
     }
     if constexpr (sizeof(C) > 1) cnt.flush(counts);
@@ -144,16 +171,19 @@ __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, c
 // lane-uniformly through the set bits of each 32-candidate chunk.
 __global__ void __launch_bounds__(256) k_row_finalize(uint32_t n, const unsigned long long* cand_off,
                                                        const float* cand_ff, const float* cand_vis,
-                                                       const uint8_t* cand_steps, const uint32_t* row_open,
-                                                       const uint32_t* row_csteps, uint32_t* row_links,
-                                                       float* row_scale, float* row_sum, float* row_sky,
-                                                       unsigned long long* row_evals) {
+                                                       const uint8_t* cand_steps, const uint16_t* clo,
+                                                       uint32_t* row_links, float* row_scale, float* row_sum,
+                                                       float* row_sky, unsigned long long* row_evals) {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
         const unsigned long long b = cand_off[row], e = cand_off[row + 1];
         float sum = 0.0f;
         uint32_t links = 0, steps = 0;
+        // The row's 16 closure rays: lanes 0..15 hold one each.
+        const uint32_t cl = lane < 16 ? clo[(size_t)row * 16 + lane] : 0u;
+        const uint32_t open = __popc(__ballot_sync(kFull, (cl & 0x100u) != 0));
+        steps = cl & 0xffu;
         for (unsigned long long base = b; base < e; base += 32) {
             unsigned long long j = base + lane;
             bool valid = j < e;
@@ -170,7 +200,7 @@ __global__ void __launch_bounds__(256) k_row_finalize(uint32_t n, const unsigned
         }
         for (int o = 16; o >= 1; o >>= 1) steps += __shfl_xor_sync(kFull, steps, o);
         if (lane == 0) {
-            float sky = (float)row_open[row] / 16.0f;
+            float sky = (float)open / 16.0f;
             float target = clampr(1.0f - sky, 0.0f, 1.0f);
             float scale = 1.0f;
             if (sum > 1e-5f) {
@@ -181,7 +211,7 @@ __global__ void __launch_bounds__(256) k_row_finalize(uint32_t n, const unsigned
             row_scale[row] = scale;
             row_sum[row] = fminf(sum, 1.0f);
             row_sky[row] = sky;
-            row_evals[row] = (unsigned long long)steps + row_csteps[row];
+            row_evals[row] = (unsigned long long)steps;
         }
     }
 }
@@ -212,35 +242,50 @@ __global__ void __launch_bounds__(256) k_row_fill(uint32_t n, const unsigned lon
     }
 }
 
-// formfactor.rs:242-253: sequential f32 sum in row order (the reference's
-// iterator sum starts from -0.0), by one thread.
-__global__ void k_mean_row_sum(uint32_t n, const uint32_t* starts, const float* row_sum, float* out_mean,
-                               unsigned long long* out_interior) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// formfactor.rs:242-253: sequential f32 sum of the interior rows' sums in
+// row order (the reference's iterator sum starts from -0.0). One CTA: all
+// threads stream chunks of rows into shared memory (rows without links
+// contribute an exact -0.0, the additive identity), thread 0 performs the
+// ordered additions; chunks are double-buffered so loads overlap the adds.
+static constexpr int kMeanBlock = 1024;
+__global__ void __launch_bounds__(kMeanBlock) k_mean_row_sum(uint32_t n, const uint32_t* starts,
+                                                               const float* row_sum, float* out_mean,
+                                                               unsigned long long* out_interior) {
+    __shared__ float buf[2][kMeanBlock];
+    __shared__ unsigned long long cnt;
+    if (threadIdx.x == 0) cnt = 0;
     float acc = -0.0f;
-    unsigned long long interior = 0;
-    uint32_t i = 0;
-    for (; i + 8 <= n; i += 8) {
-        uint32_t s[9];
-        float v[8];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) s[k] = starts[i + k];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = row_sum[i + k];
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            if (s[k + 1] > s[k]) {
-                acc += v[k];
-                ++interior;
-            }
-    }
-    for (; i < n; ++i)
-        if (starts[i + 1] > starts[i]) {
-            acc += row_sum[i];
-            ++interior;
+    const uint32_t chunks = (n + kMeanBlock - 1) / kMeanBlock;
+    unsigned long long mine = 0;
+    auto load = [&](uint32_t c, int b) {
+        uint32_t i = c * kMeanBlock + threadIdx.x;
+        float v = -0.0f;
+        if (i < n && starts[i + 1] > starts[i]) {
+            v = row_sum[i];
+            ++mine;
         }
-    *out_mean = interior ? acc / (float)interior : 0.0f;
-    *out_interior = interior;
+        buf[b][threadIdx.x] = v;
+    };
+    if (chunks) load(0, 0);
+    __syncthreads();
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const int b = c & 1;
+        if (threadIdx.x == 0) {
+#pragma unroll 16
+            for (int k = 0; k < kMeanBlock; ++k) acc += buf[b][k];
+        } else if (c + 1 < chunks) {
+            load(c + 1, b ^ 1);
+        }
+        if (threadIdx.x == 0 && c + 1 < chunks) load(c + 1, b ^ 1);
+        __syncthreads();
+    }
+    for (int o = 16; o >= 1; o >>= 1) mine += __shfl_xor_sync(kFull, mine, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&cnt, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *out_mean = cnt ? acc / (float)cnt : 0.0f;
+        *out_interior = cnt;
+    }
 }
 
 __global__ void k_sum_u64(const unsigned long long* v, uint32_t n, unsigned long long* out) {
@@ -263,33 +308,33 @@ void launch_pair_fill(cudaStream_t st, const float4* sp, const float4* sn, uint3
 void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
                        const float4* cp, const float4* cn, const uint32_t* cand_c, const uint32_t* cand_row,
                        unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status,
-                       unsigned long long* counts) {
+                       unsigned long long* counts, unsigned long long* cursor) {
     if (ncand == 0) return;
-    const unsigned g = grid_for(ncand, 128, 16);
+    const size_t sm = blob_smem(blob, 128);
     if (counts)
-        k_visibility<Counts><<<g, 128, blob_smem(blob), st>>>(blob, sc, sp, sn, cp, cn, cand_c, cand_row, ncand,
-                                                              cand_vis, cand_steps, status, counts);
+        k_visibility<Counts><<<persistent_grid(k_visibility<Counts>, 128, sm, ncand), 128, sm, st>>>(
+            blob, sc, sp, sn, cp, cn, cand_c, cand_row, ncand, cand_vis, cand_steps, status, counts, cursor);
     else
-        k_visibility<NoCount><<<g, 128, blob_smem(blob), st>>>(blob, sc, sp, sn, cp, cn, cand_c, cand_row, ncand,
-                                                               cand_vis, cand_steps, status, nullptr);
+        k_visibility<NoCount><<<persistent_grid(k_visibility<NoCount>, 128, sm, ncand), 128, sm, st>>>(
+            blob, sc, sp, sn, cp, cn, cand_c, cand_row, ncand, cand_vis, cand_steps, status, nullptr, cursor);
 }
 void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
-                    uint32_t n, uint32_t* row_open, uint32_t* row_csteps, uint32_t* status,
-                    unsigned long long* counts) {
-    const unsigned g = grid_for((unsigned long long)n * 16ull, 128, 16);
+                    uint32_t n, uint16_t* clo, uint32_t* status, unsigned long long* counts,
+                    unsigned long long* cursor) {
+    const size_t sm = blob_smem(blob, 128);
+    const unsigned long long items = (unsigned long long)n * 16ull;
     if (counts)
-        k_closure<Counts><<<g, 128, blob_smem(blob), st>>>(blob, sc, sp, sn, n, row_open, row_csteps, status, counts);
+        k_closure<Counts><<<persistent_grid(k_closure<Counts>, 128, sm, items), 128, sm, st>>>(
+            blob, sc, sp, sn, n, clo, status, counts, cursor);
     else
-        k_closure<NoCount><<<g, 128, blob_smem(blob), st>>>(blob, sc, sp, sn, n, row_open, row_csteps, status,
-                                                            nullptr);
+        k_closure<NoCount><<<persistent_grid(k_closure<NoCount>, 128, sm, items), 128, sm, st>>>(
+            blob, sc, sp, sn, n, clo, status, nullptr, cursor);
 }
 void launch_row_finalize(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const float* cand_ff,
-                         const float* cand_vis, const uint8_t* cand_steps, const uint32_t* row_open,
-                         const uint32_t* row_csteps, uint32_t* row_links, float* row_scale, float* row_sum,
-                         float* row_sky, unsigned long long* row_evals) {
+                         const float* cand_vis, const uint8_t* cand_steps, const uint16_t* clo, uint32_t* row_links,
+                         float* row_scale, float* row_sum, float* row_sky, unsigned long long* row_evals) {
     k_row_finalize<<<grid_for((unsigned long long)n * 32ull, 256), 256, 0, st>>>(
-        n, cand_off, cand_ff, cand_vis, cand_steps, row_open, row_csteps, row_links, row_scale, row_sum, row_sky,
-        row_evals);
+        n, cand_off, cand_ff, cand_vis, cand_steps, clo, row_links, row_scale, row_sum, row_sky, row_evals);
 }
 void launch_row_fill(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const uint32_t* cand_c,
                      const float* cand_ff, const float* cand_vis, const float* row_scale, const uint32_t* starts,
@@ -299,7 +344,7 @@ void launch_row_fill(cudaStream_t st, uint32_t n, const unsigned long long* cand
 }
 void launch_mean_row_sum(cudaStream_t st, uint32_t n, const uint32_t* starts, const float* row_sum,
                          float* out_mean, unsigned long long* out_interior) {
-    k_mean_row_sum<<<1, 32, 0, st>>>(n, starts, row_sum, out_mean, out_interior);
+    k_mean_row_sum<<<1, kMeanBlock, 0, st>>>(n, starts, row_sum, out_mean, out_interior);
 }
 void launch_sum_u64(cudaStream_t st, const unsigned long long* v, uint32_t n, unsigned long long* out) {
     k_sum_u64<<<grid_for(n, 256, 2), 256, 0, st>>>(v, n, out);

@@ -1,4 +1,5 @@
-// Shared kernel prologue: make the scene program visible to the CTA.
+// Shared kernel prologue: make the scene program visible to the CTA, and the
+// persistent ray-queue machinery the tracing kernels share.
 #pragma once
 
 #include "device.cuh"
@@ -6,9 +7,20 @@
 
 namespace ifx {
 
+static constexpr int kWarp = 32;
+static constexpr unsigned kFull = 0xffffffffu;
+
+// Dynamic shared memory of a tracing CTA: the staged blob (when it fits)
+// followed by the threads' BVH stacks.
+static inline size_t blob_smem(const BlobRef& b, int block) {
+    size_t s = b.staged ? (size_t)align16(b.bytes) : 0;
+    return s + (size_t)b.stack_depth * (size_t)block * 4u;
+}
+
 // Stages the blob into dynamic shared memory (one bulk copy) or, for large
-// scenes, reads it in place. All threads of the CTA must call this before
-// any of them exits. Returns false if staging timed out.
+// scenes, reads it in place, and points the view at this thread's stack.
+// All threads of the CTA must call this before any of them exits. Returns
+// false if staging timed out.
 __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsmem, uint64_t* mbar,
                                                uint32_t* status, SceneView& sv) {
     const uint8_t* base = blob.ptr;
@@ -17,6 +29,10 @@ __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsm
         base = dsmem;
     }
     sv = make_view(base);
+    uint32_t* stk = reinterpret_cast<uint32_t*>(dsmem + (blob.staged ? align16(blob.bytes) : 0u));
+    sv.stk = stk + threadIdx.x;
+    sv.stk_stride = (int)blockDim.x;
+    sv.stk_depth = blob.stack_depth;
     return true;
 }
 
@@ -26,21 +42,81 @@ __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsm
     SceneView sv;                                                             \
     if (!scene_prologue(blob, ifx_dsmem, &ifx_mbar, status, sv)) return;
 
-static inline size_t blob_smem(const BlobRef& b) { return b.staged ? b.bytes : 0; }
-
-static constexpr int kWarp = 32;
-static constexpr unsigned kFull = 0xffffffffu;
-
 // Number of CTAs for a grid-stride kernel: enough to fill every SM several
 // times over, never more than the work needs.
-static inline unsigned grid_for(unsigned long long items, int block, int per_sm_ctas = 8) {
-    int dev = 0, sms = 148;
+static inline int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = sms;
+    }
+    return cached[dev];
+}
+
+static inline unsigned grid_for(unsigned long long items, int block, int per_sm_ctas = 8) {
     unsigned long long need = (items + (unsigned long long)block - 1) / (unsigned long long)block;
-    unsigned long long cap = (unsigned long long)sms * (unsigned long long)per_sm_ctas;
+    unsigned long long cap = (unsigned long long)sm_count() * (unsigned long long)per_sm_ctas;
     if (need < 1) need = 1;
     return (unsigned)(need < cap ? need : cap);
 }
+
+// Persistent kernels: one wave of CTAs, as many as are co-resident.
+template <class K>
+static inline unsigned persistent_grid(K kernel, int block, size_t smem, unsigned long long items) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem);
+    if (per_sm < 1) per_sm = 1;
+    unsigned long long cap = (unsigned long long)sm_count() * (unsigned long long)per_sm;
+    unsigned long long need = (items + (unsigned long long)block - 1) / (unsigned long long)block;
+    if (need < 1) need = 1;
+    return (unsigned)(need < cap ? need : cap);
+}
+
+// Warp-level work distribution for persistent ray kernels. Every lane holds
+// at most one item (a ray); lanes whose ray finished are refilled from the
+// warp's private range of item indices, which is replenished in chunks of
+// kChunk indices from a global cursor with one atomic per chunk. Which lane
+// or warp traces an item never affects its result: each item's output is
+// written to a slot fixed by its index.
+struct WarpQueue {
+    static constexpr uint32_t kChunk = 256;
+    uint32_t cur, end;  // warp-uniform private range [cur, end)
+    bool drained;
+
+    __device__ __forceinline__ WarpQueue() : cur(0), end(0), drained(false) {}
+
+    // Returns the item for this lane (or ~0u) when it is idle; `idle` says
+    // whether this lane needs an item. Must be called by all 32 lanes.
+    __device__ __forceinline__ uint32_t refill(bool idle, unsigned long long total, unsigned long long* cursor) {
+        const int lane = threadIdx.x & 31;
+        unsigned need = __ballot_sync(kFull, idle);
+        uint32_t item = ~0u;
+        if (!need) return item;
+        if (cur >= end && !drained) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(cursor, (unsigned long long)kChunk);
+            base = __shfl_sync(kFull, base, 0);
+            if (base >= total) {
+                drained = true;
+            } else {
+                cur = (uint32_t)base;
+                end = (uint32_t)(base + kChunk < total ? base + kChunk : total);
+            }
+        }
+        if (cur < end) {
+            uint32_t avail = end - cur;
+            uint32_t rank = __popc(need & ((1u << lane) - 1u));
+            if (idle && rank < avail) item = cur + rank;
+            uint32_t k = __popc(need);
+            cur += k < avail ? k : avail;
+        }
+        return item;
+    }
+    __device__ __forceinline__ bool empty() const { return drained && cur >= end; }
+};
 
 }  // namespace ifx

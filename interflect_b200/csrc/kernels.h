@@ -17,6 +17,7 @@ struct BlobRef {
     const uint8_t* ptr;
     uint32_t bytes;
     int staged;
+    int stack_depth;  // BVH traversal stack entries per thread (tree depth + 2)
 };
 
 struct CamParams {
@@ -72,14 +73,14 @@ void launch_pair_fill(cudaStream_t st, const float4* sp, const float4* sn, uint3
 void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
                        const float4* cp, const float4* cn, const uint32_t* cand_c, const uint32_t* cand_row,
                        unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status,
-                       unsigned long long* counts = nullptr);
+                       unsigned long long* counts, unsigned long long* cursor);
+// clo: per (row, ray) slot (open << 8) | steps, n * 16 entries.
 void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
-                    uint32_t n, uint32_t* row_open, uint32_t* row_csteps, uint32_t* status,
-                    unsigned long long* counts = nullptr);
+                    uint32_t n, uint16_t* clo, uint32_t* status, unsigned long long* counts,
+                    unsigned long long* cursor);
 void launch_row_finalize(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const float* cand_ff,
-                         const float* cand_vis, const uint8_t* cand_steps, const uint32_t* row_open,
-                         const uint32_t* row_csteps, uint32_t* row_links, float* row_scale, float* row_sum,
-                         float* row_sky, unsigned long long* row_evals);
+                         const float* cand_vis, const uint8_t* cand_steps, const uint16_t* clo, uint32_t* row_links,
+                         float* row_scale, float* row_sum, float* row_sky, unsigned long long* row_evals);
 void launch_row_fill(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const uint32_t* cand_c,
                      const float* cand_ff, const float* cand_vis, const float* row_scale, const uint32_t* starts,
                      uint32_t* idx, float* w);
@@ -121,12 +122,23 @@ struct ShadeParams {
     int tonemap;
     const float* srgb_t;  // 256 thresholds
     float* film;          // w*h*3, nullable
-    uint8_t* out8;        // w*h*3, nullable
+    uint8_t* out8;        // w*h*3
     unsigned long long* evals;
     uint32_t* status;
     unsigned long long* counts;  // non-null: the counting instantiation (work counters, kNumCounters u64)
+    // Wavefront state, per pixel: hp = (hit point, t), hn = (normal, flags | material);
+    // per pixel and light: form factor and visibility; queues of shadow-ray
+    // slots (pixel * nl + light) and of mirror-ray pixels with their lengths
+    // qlen[0] (primary shadows), qlen[1] (mirror rays), qlen[2] (mirror-hit
+    // shadows); persistent-kernel cursors[4]. qlen and cursors start at zero.
+    float4 *hp1, *hn1, *hp2, *hn2;
+    float *ff1, *vis1, *ff2, *vis2;
+    uint32_t *q1, *q2, *qr, *qlen;
+    unsigned long long* cursors;
+    int nl;  // quad lights + sphere lights
 };
-void launch_shade(cudaStream_t st, const ShadeParams& p);
+// Returns the number of kernels launched.
+int launch_shade(cudaStream_t st, const ShadeParams& p);
 
 // Raises the dynamic shared-memory limit of every scene-staging kernel.
 void configure_surfel_kernels(int max_dyn_smem);

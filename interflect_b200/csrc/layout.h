@@ -93,6 +93,9 @@ struct SceneConsts {
     float closure[16][3];  // hemisphere_closure's fixed direction coefficients
 };
 
+#ifdef __CUDACC__
+__host__ __device__
+#endif
 static inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 
 }  // namespace ifx
