@@ -359,6 +359,92 @@ __device__ __forceinline__ float scene_dist(const SceneView& sv, V p, C& cnt) {
     return dist_mat(sv, p, cnt).d;
 }
 
+// dist_mat for a whole warp (all 32 lanes call it; lanes with !active only
+// take part in the votes). Each active lane runs its own near-first BVH
+// traversal with the reference's pruning, but leaves are evaluated in
+// warp-synchronous rounds: a lane advances through interior nodes until it
+// reaches a leaf that passes the AABB test, the warp picks one pending leaf,
+// and every lane waiting on that leaf evaluates its objects together, so the
+// primitive code runs converged. A lane's sequence of node tests, object
+// evaluations and best-distance updates is exactly the one dist_mat() makes.
+template <class C>
+__device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool active, C& cnt) {
+    DistHit best{kMaxF, 0u};
+    if (active) {
+        cnt.add(CN_SDF);
+        for (int i = 0; i < sv.n_planes; ++i) {
+            const DObject o = sv.objs[i];
+            float d = obj_dist(sv, o, p, cnt);
+            if (d < best.d) best = DistHit{d, o.mat};
+        }
+    }
+    if (!sv.use_bvh) {
+        if (active) {
+            for (int k = 0; k < sv.n_objects; ++k) {
+                const DObject o = sv.objs[sv.linear[k]];
+                float d = obj_dist(sv, o, p, cnt);
+                if (d < best.d) {
+                    best.d = d;
+                    best.mat = o.mat;
+                }
+            }
+        }
+        return best;
+    }
+    if (sv.n_nodes == 0) return best;
+    uint32_t* const stack = sv.stk;
+    const int stride = sv.stk_stride;
+    int sp = 0;
+    if (active) {
+        stack[0] = 0;
+        sp = 1;
+    }
+    int pending = -1;
+    while (true) {
+        while (pending < 0 && sp > 0) {
+            --sp;
+            const int ni = (int)stack[sp * stride];
+            const DNode nd = sv.nodes[ni];
+            if (aabb_dist(p, nd, cnt) >= best.d) continue;
+            if (nd.count > 0) {
+                pending = ni;
+                break;
+            }
+            const int l = ni + 1, r = nd.link;
+            float dl = aabb_dist(p, sv.nodes[l], cnt);
+            float dr = aabb_dist(p, sv.nodes[r], cnt);
+            if (sp + 2 > sv.stk_depth) {
+                sp = 0;
+                break;
+            }
+            if (dl < dr) {
+                stack[sp * stride] = (uint32_t)r;
+                stack[(sp + 1) * stride] = (uint32_t)l;
+            } else {
+                stack[sp * stride] = (uint32_t)l;
+                stack[(sp + 1) * stride] = (uint32_t)r;
+            }
+            sp += 2;
+        }
+        const unsigned waiting = __ballot_sync(0xffffffffu, pending >= 0);
+        if (!waiting) break;
+        const int leaf = __shfl_sync(0xffffffffu, pending, __ffs(waiting) - 1);
+        if (pending == leaf) {
+            const DNode nd = sv.nodes[leaf];
+            for (int k = nd.link; k < nd.link + nd.count; ++k) {
+                const DObject o = sv.objs[k];
+                float d = obj_dist(sv, o, p, cnt);
+                if (d < best.d) {
+                    best.d = d;
+                    best.mat = o.mat;
+                }
+            }
+            pending = -1;
+        }
+    }
+    return best;
+}
+
 // scene.rs:218-236: tetrahedron taps K = (1,-1,-1), (-1,-1,1), (-1,1,-1), (1,1,1).
 template <class C>
 __device__ __forceinline__ V scene_normal(const SceneView& sv, V p, C& cnt) {
@@ -500,6 +586,59 @@ template <class C>
 __device__ __forceinline__ int trace_step(const SceneView& sv, TraceRay& r, V& p, uint32_t& mat, C& cnt) {
     p = r.ro + r.rd * r.t;
     DistHit h = dist_mat(sv, p, cnt);
+    cnt.add(CN_TSTEP);
+    r.steps += 1;
+    float eps = 1e-4f * fmaxf(r.t, 1.0f);
+    if (h.d < eps) {
+        mat = h.mat;
+        r.steps += 4;
+        return kHit;
+    }
+    r.t += h.d;
+    if (r.t > r.tmax || r.steps >= kMaxSteps) return kMiss;
+    return kMarching;
+}
+
+// Warp-collective forms of the two steps above: all 32 lanes call them, the
+// SDF query is dist_mat_warp, and lanes with !active change nothing.
+template <class C>
+__device__ __forceinline__ bool shadow_step_w(const SceneView& sv, ShadowRay& s, bool active, float& vis, C& cnt) {
+    const float h = dist_mat_warp(sv, s.ro + s.rd * s.t, active, cnt).d;
+    if (!active) return false;
+    cnt.add(CN_SSTEP);
+    s.steps += 1;
+    if (h < 1e-4f) {
+        vis = 0.0f;
+        return true;
+    }
+    float y, d;
+    if (h < s.ph) {
+        y = h * h / (2.0f * s.ph);
+        d = sqrtf(fmaxf(h * h - y * y, 0.0f));
+    } else {
+        y = 0.0f;
+        d = h;
+    }
+    s.res = fminf(s.res, s.k * d / fmaxf(s.t - y, 1e-4f));
+    if (s.res < 1e-3f) {
+        vis = 0.0f;
+        return true;
+    }
+    s.ph = h;
+    s.t += clampr(h, 0.006f, 0.12f);
+    if (!(s.steps < kShadowSteps && s.t < s.tmax)) {
+        vis = clampr(s.res, 0.0f, 1.0f);
+        return true;
+    }
+    return false;
+}
+
+template <class C>
+__device__ __forceinline__ int trace_step_w(const SceneView& sv, TraceRay& r, bool active, V& p, uint32_t& mat,
+                                            C& cnt) {
+    p = r.ro + r.rd * r.t;
+    const DistHit h = dist_mat_warp(sv, p, active, cnt);
+    if (!active) return kMarching;
     cnt.add(CN_TSTEP);
     r.steps += 1;
     float eps = 1e-4f * fmaxf(r.t, 1.0f);

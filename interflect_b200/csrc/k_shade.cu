@@ -192,11 +192,11 @@ template <class C>
 __global__ void __launch_bounds__(128) k_primary(ShadeParams P) {
     IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
     C cnt;
-    WarpQueue q;
     const unsigned long long total = (unsigned long long)P.w * P.h;
+    WarpQueue q(total);
     const V org{P.cam.origin[0], P.cam.origin[1], P.cam.origin[2]};
     uint32_t item = ~0u;
-    TraceRay ray;
+    TraceRay ray{};
     unsigned long long ev = 0;
     while (true) {
         const uint32_t got = q.refill(item == ~0u, total, &P.cursors[0]);
@@ -208,18 +208,17 @@ __global__ void __launch_bounds__(128) k_primary(ShadeParams P) {
             if (q.empty()) break;
             continue;
         }
-        if (item != ~0u) {
-            V hp;
-            uint32_t hm = 0;
-            const int st = trace_step(sv, ray, hp, hm, cnt);
-            if (st != kMarching) {
-                ev += ray.steps;
-                const bool hit = st == kHit;
-                P.hp1[item] = make_float4(hit ? hp.x : 0.0f, hit ? hp.y : 0.0f, hit ? hp.z : 0.0f, ray.t);
-                P.hn1[item] = make_float4(__uint_as_float(ray.steps), 0.0f, 0.0f,
-                                          __uint_as_float((hit ? kFlagHit : 0u) | (hm & kMatMask)));
-                item = ~0u;
-            }
+        const bool active = item != ~0u;
+        V hp;
+        uint32_t hm = 0;
+        const int st = trace_step_w(sv, ray, active, hp, hm, cnt);
+        if (active && st != kMarching) {
+            ev += ray.steps;
+            const bool hit = st == kHit;
+            P.hp1[item] = make_float4(hit ? hp.x : 0.0f, hit ? hp.y : 0.0f, hit ? hp.z : 0.0f, ray.t);
+            P.hn1[item] = make_float4(__uint_as_float(ray.steps), 0.0f, 0.0f,
+                                      __uint_as_float((hit ? kFlagHit : 0u) | (hm & kMatMask)));
+            item = ~0u;
         }
     }
     add_evals(ev, P.evals);
@@ -298,10 +297,10 @@ __global__ void __launch_bounds__(128) k_shadow(ShadeParams P, const float4* hp,
                                                  unsigned long long* cursor) {
     IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
     C cnt;
-    WarpQueue q;
     const unsigned long long total = *qlen;
+    WarpQueue q(total);
     uint32_t item = ~0u;
-    ShadowRay ray;
+    ShadowRay ray{};
     unsigned long long ev = 0;
     while (true) {
         const uint32_t got = q.refill(item == ~0u, total, cursor);
@@ -323,13 +322,12 @@ __global__ void __launch_bounds__(128) k_shadow(ShadeParams P, const float4* hp,
             if (q.empty()) break;
             continue;
         }
-        if (item != ~0u) {
-            float vis;
-            if (shadow_step(sv, ray, vis, cnt)) {
-                vis_out[item] = vis;
-                ev += ray.steps;
-                item = ~0u;
-            }
+        const bool active = item != ~0u;
+        float vis;
+        if (shadow_step_w(sv, ray, active, vis, cnt) && active) {
+            vis_out[item] = vis;
+            ev += ray.steps;
+            item = ~0u;
         }
     }
     add_evals(ev, P.evals);
@@ -341,10 +339,10 @@ template <class C>
 __global__ void __launch_bounds__(128) k_reflect(ShadeParams P) {
     IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
     C cnt;
-    WarpQueue q;
     const unsigned long long total = P.qlen[1];
+    WarpQueue q(total);
     uint32_t item = ~0u, pix = 0;
-    TraceRay ray;
+    TraceRay ray{};
     unsigned long long ev = 0;
     while (true) {
         const uint32_t got = q.refill(item == ~0u, total, &P.cursors[1]);
@@ -360,17 +358,16 @@ __global__ void __launch_bounds__(128) k_reflect(ShadeParams P) {
             if (q.empty()) break;
             continue;
         }
-        if (item != ~0u) {
-            V hp;
-            uint32_t hm = 0;
-            const int st = trace_step(sv, ray, hp, hm, cnt);
-            if (st != kMarching) {
-                ev += ray.steps;
-                const bool hit = st == kHit;
-                P.hp2[pix] = make_float4(hit ? hp.x : 0.0f, hit ? hp.y : 0.0f, hit ? hp.z : 0.0f, ray.t);
-                P.hn2[pix] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float((hit ? kFlagHit : 0u) | (hm & kMatMask)));
-                item = ~0u;
-            }
+        const bool active = item != ~0u;
+        V hp;
+        uint32_t hm = 0;
+        const int st = trace_step_w(sv, ray, active, hp, hm, cnt);
+        if (active && st != kMarching) {
+            ev += ray.steps;
+            const bool hit = st == kHit;
+            P.hp2[pix] = make_float4(hit ? hp.x : 0.0f, hit ? hp.y : 0.0f, hit ? hp.z : 0.0f, ray.t);
+            P.hn2[pix] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float((hit ? kFlagHit : 0u) | (hm & kMatMask)));
+            item = ~0u;
         }
     }
     add_evals(ev, P.evals);

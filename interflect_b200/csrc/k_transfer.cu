@@ -83,10 +83,10 @@ __global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc
                                                      unsigned long long* counts, unsigned long long* cursor) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
     C cnt;
-    WarpQueue q;
+    WarpQueue q(ncand);
     const float off = sc.diag * 5e-4f, tmin = sc.diag * 1e-3f;
     uint32_t item = ~0u;
-    ShadowRay ray;
+    ShadowRay ray{};
     while (true) {
         const uint32_t got = q.refill(item == ~0u, ncand, cursor);
         if (got != ~0u) {
@@ -109,13 +109,12 @@ __global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc
             if (q.empty()) break;
             continue;
         }
-        if (item != ~0u) {
-            float vis;
-            if (shadow_step(sv, ray, vis, cnt)) {
-                cand_vis[item] = vis;
-                cand_steps[item] = (uint8_t)ray.steps;
-                item = ~0u;
-            }
+        const bool active = item != ~0u;
+        float vis;
+        if (shadow_step_w(sv, ray, active, vis, cnt) && active) {
+            cand_vis[item] = vis;
+            cand_steps[item] = (uint8_t)ray.steps;
+            item = ~0u;
         }
     }
     if constexpr (sizeof(C) > 1) cnt.flush(counts);
@@ -132,11 +131,11 @@ __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, c
                                                   unsigned long long* counts, unsigned long long* cursor) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
     C cnt;
-    WarpQueue q;
     const unsigned long long total = (unsigned long long)n * 16ull;
+    WarpQueue q(total);
     const float tmax = sc.diag * 2.0f;
     uint32_t item = ~0u;
-    TraceRay ray;
+    TraceRay ray{};
     while (true) {
         const uint32_t got = q.refill(item == ~0u, total, cursor);
         if (got != ~0u) {
@@ -152,14 +151,13 @@ __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, c
             if (q.empty()) break;
             continue;
         }
-        if (item != ~0u) {
-            V hp;
-            uint32_t hm;
-            const int st = trace_step(sv, ray, hp, hm, cnt);
-            if (st != kMarching) {
-                clo[item] = (uint16_t)(((st == kMiss) ? 0x100u : 0u) | ray.steps);
-                item = ~0u;
-            }
+        const bool active = item != ~0u;
+        V hp;
+        uint32_t hm;
+        const int st = trace_step_w(sv, ray, active, hp, hm, cnt);
+        if (active && st != kMarching) {
+            clo[item] = (uint16_t)(((st == kMiss) ? 0x100u : 0u) | ray.steps);
+            item = ~0u;
         }
     }
     if constexpr (sizeof(C) > 1) cnt.flush(counts);

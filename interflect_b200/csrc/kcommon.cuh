@@ -83,11 +83,17 @@ static inline unsigned persistent_grid(K kernel, int block, size_t smem, unsigne
 // or warp traces an item never affects its result: each item's output is
 // written to a slot fixed by its index.
 struct WarpQueue {
-    static constexpr uint32_t kChunk = 256;
     uint32_t cur, end;  // warp-uniform private range [cur, end)
+    uint32_t kChunk;    // items taken per atomic: about 1/8 of a fair share per warp, 32..256
     bool drained;
 
-    __device__ __forceinline__ WarpQueue() : cur(0), end(0), drained(false) {}
+    __device__ __forceinline__ WarpQueue() : cur(0), end(0), kChunk(32), drained(false) {}
+    __device__ __forceinline__ explicit WarpQueue(unsigned long long total) : cur(0), end(0), drained(false) {
+        const unsigned long long warps = (unsigned long long)gridDim.x * blockDim.x / 32u;
+        unsigned long long c = total / (warps * 8ull + 1ull);
+        c = c < 32ull ? 32ull : (c > 256ull ? 256ull : c);
+        kChunk = (uint32_t)(c & ~31ull);
+    }
 
     // Returns the item for this lane (or ~0u) when it is idle; `idle` says
     // whether this lane needs an item. Must be called by all 32 lanes.
