@@ -203,6 +203,46 @@ int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals);
  * max_bounces is reached. */
 int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* out);
 
+/* Largest cluster count ifx_solve_noalloc accepts. */
+#define IFX_NOALLOC_MAX_CLUSTERS 16384
+
+/* The Jacobi solve without any allocation; it has no counterpart in the
+ * reference. For callers that cannot let a library allocate GPU memory: a
+ * host engine that reserves the device up front and serves memory only from
+ * its own arena, a frame loop that must not stall on cudaMalloc's implicit
+ * synchronisation, or a binding whose buffers belong to another runtime.
+ * It runs the same bounce kernels as ifx_solve on device buffers the caller
+ * owns and calls no cudaMalloc, cudaFree or allocating library routine. Its
+ * scratch (a radiosity value per cluster and a control block) is one static
+ * device array of IFX_NOALLOC_MAX_CLUSTERS * 16 + 256 bytes that every GPU
+ * loading this library holds until the process exits; nc above
+ * IFX_NOALLOC_MAX_CLUSTERS is rejected with IFX_ERR_LIMIT.
+ *
+ * All array arguments are DEVICE pointers on `device`, as float4 / uint2
+ * records (16 / 8 bytes per element):
+ *   p_area4          n   surfel position, w = area (read)
+ *   direct4, albedo4 n   E and diffuse albedo (read)
+ *   irr4, rad4       n   irradiance and radiosity; rad4 holds the initial B
+ *                        (E after ifx_light_surfels) and both are written
+ *   cluster_p_area4  nc  cluster position, w = area (read)
+ *   cluster_ranges   nc  [begin, end) of each cluster in `members` (uint2)
+ *   members, starts, idx, w   cluster members and the CSR matrix (read)
+ * `stream` is a cudaStream_t (NULL: the default stream). The call returns
+ * after the solve has finished on that stream.
+ *
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. Every call shares the one array and it keeps
+ * the last call's contents (the control block is cleared at the start of
+ * each call): calls whose work overlaps on the GPU race, so serialise them.
+ * Errors are reported as in the rest of this API, with the message written
+ * to `err` (nullable). Follows solve.rs:47-108. */
+int ifx_solve_noalloc(int device, void* stream, uint32_t n, uint32_t nc, const float* p_area4, const float* direct4,
+                      const float* albedo4, float* irr4, float* rad4, const float* cluster_p_area4,
+                      const uint32_t* cluster_ranges, const uint32_t* members, const uint32_t* starts,
+                      const uint32_t* idx, const float* w, uint32_t max_bounces, ifx_solve_stats* out, char* err,
+                      size_t errlen);
+
 /* ------------------------------------------------------------- shade --- */
 
 /* Replaces surfel::Grid::build (src/surfel.rs:71-114) with the gather radius

@@ -43,7 +43,9 @@ EXPORTS = (
     "ifx_transfer_build", "ifx_transfer_download", "ifx_clusters_download", "ifx_transfer_row_diag",
     "ifx_transfer_upload", "ifx_light_surfels", "ifx_solve", "ifx_grid_build", "ifx_render_frame",
     "ifx_set_work_counting", "ifx_reset_work", "ifx_get_work", "ifx_timer_start", "ifx_timer_stop",
+    "ifx_solve_noalloc",
 )
+NOALLOC_MAX_CLUSTERS = 16384
 KERNELS = {"visibility": 0, "closure": 1, "light": 2, "shade": 3}
 WORK_COUNTERS = 21
 
@@ -133,6 +135,8 @@ def lib() -> C.CDLL:
         "ifx_get_work": (I, [P, I, P, C.POINTER(C.c_double)]),
         "ifx_timer_start": (I, [P]),
         "ifx_timer_stop": (I, [P, C.POINTER(F)]),
+        "ifx_solve_noalloc": (I, [I, P, U32, U32, P, P, P, P, P, P, P, P, P, P, P, U32, C.POINTER(_SolveStats),
+                                  C.c_char_p, C.c_size_t]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -426,6 +430,26 @@ class Context:
         ms = C.c_float()
         self._check(lib().ifx_timer_stop(self._h, C.byref(ms)), "timer_stop")
         return ms.value
+
+
+def solve_noalloc(device: int, stream: int, n: int, nc: int, p_area4: int, direct4: int, albedo4: int, irr4: int,
+                  rad4: int, cluster_p_area4: int, cluster_ranges: int, members: int, starts: int, idx: int, w: int,
+                  max_bounces: int) -> SolveStats:
+    """The Jacobi solve on caller-owned device buffers (integer device
+    addresses) with no allocation by the library, for callers that cannot
+    let it allocate GPU memory (see ifx_solve_noalloc in interflect.h for the
+    layouts and the IFX_NOALLOC_MAX_CLUSTERS limit). Raises LimitError above
+    that limit and DeviceError on CUDA failures."""
+    st = _SolveStats()
+    err = C.create_string_buffer(256)
+    r = lib().ifx_solve_noalloc(device, stream or None, n, nc, p_area4, direct4, albedo4, irr4, rad4,
+                                cluster_p_area4, cluster_ranges, members, starts, idx, w, max_bounces,
+                                C.byref(st), err, 256)
+    if r == IFX_ERR_LIMIT:
+        raise LimitError(err.value.decode())
+    if r != IFX_OK:
+        raise DeviceError(f"ifx_solve_noalloc failed ({r}): {err.value.decode()}")
+    return SolveStats(st.iterations, st.residual)
 
 
 def cuda_available() -> bool:
