@@ -102,13 +102,22 @@ typedef struct ifx_stats {
     uint64_t kernel_launches;  /* kernels this context has launched so far */
     float ms_transfer, ms_light, ms_solve, ms_grid, ms_shade; /* CUDA-event times of the last call of each stage */
     float ms_visibility, ms_closure; /* CUDA-event times of the last visibility and closure kernels */
+    /* CUDA-event times of the last frame's shading kernels: camera rays,
+     * shadow cones of the camera hits, mirror rays, shadow cones of the
+     * mirror hits, and the rest (setup, mirror setup, compose + encode). */
+    float ms_primary, ms_shadow, ms_reflect, ms_shadow2, ms_shade_other;
 } ifx_stats;
 
-/* Tracing kernels, for work accounting. */
+/* Kernels, for work accounting (ifx_get_work). */
 #define IFX_KERNEL_VISIBILITY 0
 #define IFX_KERNEL_CLOSURE 1
 #define IFX_KERNEL_LIGHT 2
-#define IFX_KERNEL_SHADE 3
+#define IFX_KERNEL_PRIMARY 3
+#define IFX_KERNEL_SHADOW 4
+#define IFX_KERNEL_REFLECT 5
+#define IFX_KERNEL_SHADOW2 6
+#define IFX_KERNEL_SHADE_OTHER 7
+#define IFX_NUM_KERNELS 8
 #define IFX_WORK_COUNTERS 21
 
 /* ------------------------------------------------------------- scene --- */

@@ -46,7 +46,8 @@ EXPORTS = (
     "ifx_solve_noalloc",
 )
 NOALLOC_MAX_CLUSTERS = 16384
-KERNELS = {"visibility": 0, "closure": 1, "light": 2, "shade": 3}
+KERNELS = {"visibility": 0, "closure": 1, "light": 2, "primary": 3, "shadow": 4, "reflect": 5, "shadow2": 6,
+           "shade_other": 7}
 WORK_COUNTERS = 21
 
 
@@ -90,7 +91,9 @@ class _SolveStats(C.Structure):
 class _Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_uint64), ("ms_transfer", C.c_float), ("ms_light", C.c_float),
                 ("ms_solve", C.c_float), ("ms_grid", C.c_float), ("ms_shade", C.c_float),
-                ("ms_visibility", C.c_float), ("ms_closure", C.c_float)]
+                ("ms_visibility", C.c_float), ("ms_closure", C.c_float), ("ms_primary", C.c_float),
+                ("ms_shadow", C.c_float), ("ms_reflect", C.c_float), ("ms_shadow2", C.c_float),
+                ("ms_shade_other", C.c_float)]
 
 
 _lib_handle = None

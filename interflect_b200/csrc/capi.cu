@@ -88,6 +88,7 @@ struct ifx_ctx {
 
     // measurement: per-kernel events, work counters (4 kernels x 21 u64), timer
     cudaEvent_t kv0 = nullptr, kv1 = nullptr, kc0 = nullptr, kc1 = nullptr, tm0 = nullptr, tm1 = nullptr;
+    cudaEvent_t shev[kShadeEvents] = {};
     bool counting = false;
     DBuf work;
     void* pinned = nullptr;  // upload staging (page-locked)
@@ -294,8 +295,10 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
     if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) return bail(e);
     for (cudaEvent_t* ev : {&ctx->kv0, &ctx->kv1, &ctx->kc0, &ctx->kc1, &ctx->tm0, &ctx->tm1})
         if ((e = cudaEventCreate(ev)) != cudaSuccess) return bail(e);
-    if (ensure(ctx, ctx->work, 4 * IFX_WORK_COUNTERS * 8) != IFX_OK ||
-        cudaMemsetAsync(ctx->work.p, 0, 4 * IFX_WORK_COUNTERS * 8, ctx->st) != cudaSuccess)
+    for (int i = 0; i < kShadeEvents; ++i)
+        if ((e = cudaEventCreate(&ctx->shev[i])) != cudaSuccess) return bail(e);
+    if (ensure(ctx, ctx->work, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8) != IFX_OK ||
+        cudaMemsetAsync(ctx->work.p, 0, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8, ctx->st) != cudaSuccess)
         return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->qcur, 16 * 8) != IFX_OK || ensure(ctx, ctx->qlen, 16) != IFX_OK)
         return bail(cudaErrorMemoryAllocation);
@@ -332,6 +335,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
         if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ctx->shev)
+        if (ev) cudaEventDestroy(ev);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }
@@ -354,13 +359,13 @@ extern "C" int ifx_set_work_counting(ifx_ctx* ctx, int on) {
 extern "C" int ifx_reset_work(ifx_ctx* ctx) {
     if (!ctx) return IFX_ERR_INVALID;
     CK(cudaSetDevice(ctx->device));
-    CK(cudaMemsetAsync(ctx->work.p, 0, 4 * IFX_WORK_COUNTERS * 8, ctx->st));
+    CK(cudaMemsetAsync(ctx->work.p, 0, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return IFX_OK;
 }
 
 extern "C" int ifx_get_work(ifx_ctx* ctx, int kernel, uint64_t* counts, double* flops) {
-    if (!ctx || kernel < 0 || kernel > 3) return fail(ctx, IFX_ERR_INVALID, "bad kernel id");
+    if (!ctx || kernel < 0 || kernel >= IFX_NUM_KERNELS) return fail(ctx, IFX_ERR_INVALID, "bad kernel id");
     CK(cudaSetDevice(ctx->device));
     unsigned long long h[IFX_WORK_COUNTERS];
     CK(cudaMemcpyAsync(h, (unsigned long long*)ctx->work.p + (size_t)kernel * IFX_WORK_COUNTERS, sizeof h,
@@ -1044,7 +1049,7 @@ extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, u
     unsigned long long* small = (unsigned long long*)ctx->small.p;
     P.evals = &small[3];
     P.status = (uint32_t*)ctx->status.p;
-    P.counts = ctx->work_of(IFX_KERNEL_SHADE);
+    P.counts = ctx->work_of(IFX_KERNEL_PRIMARY);  // slots PRIMARY..SHADE_OTHER
     // Wavefront buffers (grow-only).
     const int nl = (int)(s.lights.size() + s.sphere_lights.size());
     const size_t slots = px * (size_t)(nl > 0 ? nl : 1);
@@ -1077,7 +1082,7 @@ extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, u
     CK(cudaMemsetAsync(ctx->qlen.p, 0, 16, ctx->st));
     CK(cudaMemsetAsync(ctx->qcur.p, 0, 16 * 8, ctx->st));
     CK(cudaEventRecord(ctx->ev0, ctx->st));
-    ctx->launches += (uint64_t)launch_shade(ctx->st, P);
+    ctx->launches += (uint64_t)launch_shade(ctx->st, P, ctx->shev);
     CKL();
     CK(cudaEventRecord(ctx->ev1, ctx->st));
     unsigned long long e = 0;
@@ -1087,6 +1092,13 @@ extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, u
     int r = check_status(ctx);
     if (r) return r;
     CK(cudaEventElapsedTime(&ctx->stats.ms_shade, ctx->ev0, ctx->ev1));
+    float g[7];
+    for (int i = 0; i < 7; ++i) CK(cudaEventElapsedTime(&g[i], ctx->shev[2 * i], ctx->shev[2 * i + 1]));
+    ctx->stats.ms_primary = g[0];
+    ctx->stats.ms_shadow = g[1];
+    ctx->stats.ms_reflect = g[2];
+    ctx->stats.ms_shadow2 = g[3];
+    ctx->stats.ms_shade_other = g[4] + g[5] + g[6];
     if (evals) *evals = e;
     return IFX_OK;
 }

@@ -467,28 +467,54 @@ __global__ void __launch_bounds__(128) k_compose(ShadeParams P) {
     if constexpr (sizeof(C) > 1) cnt.flush(P.counts);
 }
 
+// ev (nullable): kShadeEvents events recorded around the kernels, in
+// pairs: [0,1] primary, [2,3] shadow, [4,5] reflect, [6,7] shadow2, and the
+// rest as [8,9] setup, [10,11] setup2, [12,13] compose. Work counters go to
+// slots (kNumCounters u64 each) 0 primary, 1 shadow, 2 reflect, 3 shadow2,
+// 4 the rest.
 template <class C>
-static void launch_all(cudaStream_t st, const ShadeParams& p) {
+static void launch_all(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev) {
     const size_t sm = blob_smem(p.blob, 128);
     const unsigned long long px = (unsigned long long)p.w * p.h;
     const unsigned long long slots = px * (unsigned long long)(p.nl > 0 ? p.nl : 1);
-    k_primary<C><<<persistent_grid(k_primary<C>, 128, sm, px), 128, sm, st>>>(p);
-    k_setup<C><<<grid_for(px, 128, 16), 128, sm, st>>>(p);
-    k_shadow<C><<<persistent_grid(k_shadow<C>, 128, sm, slots), 128, sm, st>>>(p, p.hp1, p.hn1, p.q1, &p.qlen[0],
-                                                                                p.vis1, &p.cursors[2]);
-    if (p.has_gi) {
-        k_reflect<C><<<persistent_grid(k_reflect<C>, 128, sm, px), 128, sm, st>>>(p);
-        k_setup2<C><<<grid_for(px, 128, 16), 128, sm, st>>>(p);
-        k_shadow<C><<<persistent_grid(k_shadow<C>, 128, sm, slots), 128, sm, st>>>(p, p.hp2, p.hn2, p.q2,
+    auto with = [&](int slot) {
+        ShadeParams q = p;
+        q.counts = p.counts ? p.counts + (size_t)slot * kNumCounters : nullptr;
+        return q;
+    };
+    auto rec = [&](int i) {
+        if (ev) cudaEventRecord(ev[i], st);
+    };
+    rec(0);
+    k_primary<C><<<persistent_grid(k_primary<C>, 128, sm, px), 128, sm, st>>>(with(0));
+    rec(1);
+    rec(8);
+    k_setup<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
+    rec(9);
+    rec(2);
+    k_shadow<C><<<persistent_grid(k_shadow<C>, 128, sm, slots), 128, sm, st>>>(with(1), p.hp1, p.hn1, p.q1,
+                                                                                &p.qlen[0], p.vis1, &p.cursors[2]);
+    rec(3);
+    rec(4);
+    if (p.has_gi) k_reflect<C><<<persistent_grid(k_reflect<C>, 128, sm, px), 128, sm, st>>>(with(2));
+    rec(5);
+    rec(10);
+    if (p.has_gi) k_setup2<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
+    rec(11);
+    rec(6);
+    if (p.has_gi)
+        k_shadow<C><<<persistent_grid(k_shadow<C>, 128, sm, slots), 128, sm, st>>>(with(3), p.hp2, p.hn2, p.q2,
                                                                                     &p.qlen[2], p.vis2,
                                                                                     &p.cursors[3]);
-    }
-    k_compose<C><<<grid_for(px, 128, 16), 128, sm, st>>>(p);
+    rec(7);
+    rec(12);
+    k_compose<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
+    rec(13);
 }
 
-int launch_shade(cudaStream_t st, const ShadeParams& p) {
-    if (p.counts) launch_all<Counts>(st, p);
-    else launch_all<NoCount>(st, p);
+int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev) {
+    if (p.counts) launch_all<Counts>(st, p, ev);
+    else launch_all<NoCount>(st, p, ev);
     return p.has_gi ? 7 : 4;
 }
 

@@ -137,8 +137,11 @@ struct ShadeParams {
     unsigned long long* cursors;
     int nl;  // quad lights + sphere lights
 };
-// Returns the number of kernels launched.
-int launch_shade(cudaStream_t st, const ShadeParams& p);
+// Returns the number of kernels launched. `ev` (nullable) holds
+// kShadeEvents events recorded around the kernels (see k_shade.cu);
+// p.counts (nullable) points at 5 consecutive counter slots.
+static constexpr int kShadeEvents = 14;
+int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev);
 
 // Raises the dynamic shared-memory limit of every scene-staging kernel.
 void configure_surfel_kernels(int max_dyn_smem);
