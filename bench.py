@@ -39,7 +39,11 @@ WORKLOADS = {
     "c1_cornell": ("interflect_b200/scenes/c1_cornell.rad", "Cornell box 260x260, 20k surfels, 12 bounces"),
     "c3_stress": ("interflect_b200/scenes/c3_stress.rad",
                   "512 primitives, 3840x2160, 1M surfels requested, 24 bounces"),
+    "c4_batch": ("interflect_b200/scenes/c1_cornell.rad",
+                 "256 relighting right-hand sides (1-4 surfels-as-lights, intensity U[1,50]) on the Cornell "
+                 "transfer, one CSR SpMM solve, 12 bounces max"),
 }
+BATCH_METRIC = "relighting solves per second (256 right-hand sides on one transfer matrix)"
 METRIC = "SDF evaluations per second, one full frame (transfer + light + solve + grid + shade)"
 # Kernels with per-launch CUDA-event times and work counters (the ray-marching
 # kernels, plus the shade stage's setup/compose kernels as one group).
@@ -294,6 +298,81 @@ def run_ours(args, world, rank, local) -> dict | None:
     return line
 
 
+def relight_rhs(n: int, R: int, seed: int = 7):
+    """R emission vectors, each 1-4 surfels-as-lights of intensity U[1, 50]."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    E = np.zeros((R, n, 3), np.float32)
+    for r in range(R):
+        k = rng.integers(1, 5)
+        idx = rng.choice(n, size=k, replace=False)
+        E[r, idx, :] = rng.uniform(1.0, 50.0, size=(k, 1)).astype(np.float32)
+    return E
+
+
+def run_batch(args, world, rank, local) -> dict | None:
+    """Batched relighting: solves/s of the SpMM path against a plain loop of
+    single-RHS solves through the same API, both on this GPU."""
+    import interflect_b200 as ifx
+    scene_path, desc = WORKLOADS[args.workload]
+    with open(os.path.join(ROOT, scene_path)) as f:
+        src = f.read()
+    scene = ifx.parse(src)
+    ctx = ifx.Context(local)
+    ctx.upload(scene)
+    placed = ctx.generate(scene.cfg.surfels)
+    info = ctx.build(8)
+    R, bounces = 256, scene.cfg.bounces
+    E = relight_rhs(placed, R)
+    tuned = ctx.autotune_batched(E)
+    ctx.solve_batched(E, bounces, outputs=False)  # leaves E resident
+    for _ in range(args.warmup):
+        ctx.solve_batched(None, bounces, outputs=False, R=R)
+    flusher = L2Flusher(local)
+    barrier(world)
+    launches0 = ctx.stats()["kernel_launches"]
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flusher.flush()
+        ctx.timer_start()
+        _, _, its, _ = ctx.solve_batched(None, bounces, outputs=False, R=R)
+        total_ms += ctx.timer_stop()
+    launches = ctx.stats()["kernel_launches"] - launches0
+    # End to end: right-hand sides from host memory, radiosity back to host.
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flusher.flush()
+        ctx.timer_start()
+        ctx.solve_batched(E, bounces, outputs=True)
+        e2e_ms += ctx.timer_stop()
+    # Baseline: the plain loop of single-RHS solves through the public API.
+    loop_n = min(R, 32)
+    ctx.timer_start()
+    for r in range(loop_n):
+        ctx.set_emission(E[r])
+        ctx.solve(bounces)
+    loop_ms = ctx.timer_stop()
+    (t_max, e2e_max), _ = allreduce_max_sum([total_ms, e2e_ms], [0.0], world)
+    if rank != 0:
+        return None
+    value = R * args.steps * world / (t_max / 1e3)
+    loop_rate = loop_n / (loop_ms / 1e3)
+    return {
+        "metric": BATCH_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "scene": scene_path, "description": desc, "surfels_placed": placed,
+                   "clusters": info.clusters, "links": info.links, "rhs": R, "max_bounces": bounces,
+                   "bounces_run_max": int(max(its)), "spmm_warps_per_block": tuned,
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "plain_loop": {"value": loop_rate, "unit": "solves/s", "rhs_timed": loop_n,
+                       "speedup": value / loop_rate},
+        "e2e": {"value": R * args.steps / (e2e_max / 1e3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(E.nbytes), "d2h_bytes_per_step": int(2 * E.nbytes)},
+        "gpu_launches": int(launches),
+    }
+
+
 def cpu_frame(src, surf, cfg, threads, rows_frac=1.0):
     """One frame of the oracle (the reference algorithm on the CPU) on the
     given surfels; shading restricted to the first rows_frac of the rows."""
@@ -386,7 +465,12 @@ def main():
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()
     try:
-        line = run_reference(args, world, rank) if args.impl == "reference" else run_ours(args, world, rank, local)
+        if args.impl == "reference":
+            line = run_reference(args, world, rank)
+        elif args.workload == "c4_batch":
+            line = run_batch(args, world, rank, local)
+        else:
+            line = run_ours(args, world, rank, local)
         if line is not None:
             print(json.dumps(line), flush=True)
     finally:

@@ -212,6 +212,26 @@ int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals);
  * max_bounces is reached. */
 int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* out);
 
+/* Relighting: installs an emission vector E (host, n x 3) as the solve's
+ * source, i.e. direct = rad = E and irr = 0, the state solve::light_surfels
+ * leaves (solve.rs:30-36) with E given instead of computed. */
+int ifx_surfels_set_emission(ifx_ctx* ctx, const float* E);
+
+/* Batched relighting: R right-hand sides E (host, R x n x 3, one emission
+ * vector per rhs) solved on the current transfer matrix as a CSR SpMM. Each
+ * rhs runs solve::solve (solve.rs:47-108) with its own stop rule and is
+ * bit-identical to ifx_surfels_set_emission(E_r) + ifx_solve. E may be
+ * NULL to reuse the right-hand sides of the previous call (resident on the
+ * device; same R and n). Outputs (all nullable): rad and irr as R x n x 3,
+ * iterations and residual per rhs. */
+int ifx_solve_batched(ifx_ctx* ctx, uint32_t R, const float* E, uint32_t max_bounces, float* rad_out,
+                      float* irr_out, uint32_t* iterations, float* residual);
+/* Times ifx_solve_batched's SpMM block shapes (2, 4, 8, 16 warps of rows
+ * per block) on the current matrix with R right-hand sides of E and keeps
+ * the fastest for later calls; the choice never changes results. `best`
+ * receives the chosen warps per block (nullable). */
+int ifx_autotune_batched(ifx_ctx* ctx, uint32_t R, const float* E, int* best);
+
 /* Largest cluster count ifx_solve_noalloc accepts. */
 #define IFX_NOALLOC_MAX_CLUSTERS 16384
 

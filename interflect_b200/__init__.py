@@ -43,7 +43,7 @@ EXPORTS = (
     "ifx_transfer_build", "ifx_transfer_download", "ifx_clusters_download", "ifx_transfer_row_diag",
     "ifx_transfer_upload", "ifx_light_surfels", "ifx_solve", "ifx_grid_build", "ifx_render_frame",
     "ifx_set_work_counting", "ifx_reset_work", "ifx_get_work", "ifx_timer_start", "ifx_timer_stop",
-    "ifx_solve_noalloc",
+    "ifx_solve_noalloc", "ifx_surfels_set_emission", "ifx_solve_batched", "ifx_autotune_batched",
 )
 NOALLOC_MAX_CLUSTERS = 16384
 KERNELS = {"visibility": 0, "closure": 1, "light": 2, "primary": 3, "shadow": 4, "reflect": 5, "shadow2": 6,
@@ -140,6 +140,9 @@ def lib() -> C.CDLL:
         "ifx_timer_stop": (I, [P, C.POINTER(F)]),
         "ifx_solve_noalloc": (I, [I, P, U32, U32, P, P, P, P, P, P, P, P, P, P, P, U32, C.POINTER(_SolveStats),
                                   C.c_char_p, C.c_size_t]),
+        "ifx_surfels_set_emission": (I, [P, P]),
+        "ifx_solve_batched": (I, [P, U32, P, U32, P, P, P, P]),
+        "ifx_autotune_batched": (I, [P, U32, P, C.POINTER(I)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -389,6 +392,35 @@ class Context:
         s = _SolveStats()
         self._check(lib().ifx_solve(self._h, max_bounces, C.byref(s)), "solve")
         return SolveStats(s.iterations, s.residual)
+
+    # -- relighting -----------------------------------------------------------
+    def set_emission(self, E) -> None:
+        """direct = rad = E, irr = 0: the solve's source for one relighting."""
+        E = np.ascontiguousarray(E, np.float32).reshape(-1, 3)
+        self._check(lib().ifx_surfels_set_emission(self._h, _ptr(E)), "set_emission")
+
+    def solve_batched(self, E, max_bounces: int, outputs: bool = True, R: int | None = None):
+        """R relighting right-hand sides E (R x n x 3) as one SpMM solve; E
+        None reuses the previous call's right-hand sides (resident on the
+        device; pass R). Returns (rad R x n x 3, irr R x n x 3, iterations[R],
+        residual[R]); rad and irr are None when outputs is False."""
+        if E is not None:
+            E = np.ascontiguousarray(E, np.float32)
+            R = E.shape[0]
+        shape = (R, self.n_surfels, 3)
+        rad = np.zeros(shape, np.float32) if outputs else None
+        irr = np.zeros(shape, np.float32) if outputs else None
+        it = np.zeros(R, np.uint32)
+        res = np.zeros(R, np.float32)
+        self._check(lib().ifx_solve_batched(self._h, R, _ptr(E), max_bounces, _ptr(rad), _ptr(irr), _ptr(it),
+                                            _ptr(res)), "solve_batched")
+        return rad, irr, it, res
+
+    def autotune_batched(self, E) -> int:
+        E = np.ascontiguousarray(E, np.float32)
+        best = C.c_int()
+        self._check(lib().ifx_autotune_batched(self._h, E.shape[0], _ptr(E), C.byref(best)), "autotune_batched")
+        return best.value
 
     # -- shade --------------------------------------------------------------
     def grid_build(self, radius: float = 0.0) -> None:

@@ -72,6 +72,11 @@ struct ifx_ctx {
     // solve
     DBuf cluster_rad, ctl;
 
+    // batched relighting
+    DBuf bE, bdirect, brad, birr, bcrad, bdone, biters, bres, blast, bunpack;
+    int spmm_warps = 8;
+    uint32_t bE_n = 0, bE_R = 0;  // shape of the right-hand sides resident in bE
+
     // grid
     bool has_grid = false;
     GridParams grid{};
@@ -330,7 +335,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->row_scale, &ctx->row_sum, &ctx->row_sky, &ctx->row_evals, &ctx->starts, &ctx->idx,
                     &ctx->w, &ctx->cluster_rad, &ctx->ctl, &ctx->gkeys, &ctx->gkeys_alt, &ctx->gstarts, &ctx->gp,
                     &ctx->gn, &ctx->girr, &ctx->gitems, &ctx->film, &ctx->out8, &ctx->cub_tmp, &ctx->small,
-                    &ctx->gen_cand, &ctx->work};
+                    &ctx->gen_cand, &ctx->work, &ctx->bE, &ctx->bdirect, &ctx->brad, &ctx->birr, &ctx->bcrad,
+                    &ctx->bdone, &ctx->biters, &ctx->bres, &ctx->blast, &ctx->bunpack};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -939,6 +945,122 @@ extern "C" int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* ou
         memcpy(&res, &h.last_residual, 4);
         out->residual = res;
     }
+    return IFX_OK;
+}
+
+// ------------------------------------------------------------ relighting ---
+extern "C" int ifx_surfels_set_emission(ifx_ctx* ctx, const float* E) {
+    if (!ctx || !E) return fail(ctx, IFX_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    const uint32_t n = ctx->n;
+    std::vector<float4> h(n);
+    for (uint32_t i = 0; i < n; ++i) h[i] = make_float4(E[3 * i], E[3 * i + 1], E[3 * i + 2], 0.0f);
+    if (n) {
+        CK(cudaMemcpyAsync(ctx->sdir.p, h.data(), (size_t)n * 16, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->srad.p, h.data(), (size_t)n * 16, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemsetAsync(ctx->sirr.p, 0, (size_t)n * 16, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->has_grid = false;
+    return IFX_OK;
+}
+
+// Uploads E and runs the batched bounces; outputs stay on the device.
+static int batched_run(ifx_ctx* ctx, uint32_t R, const float* E, uint32_t max_bounces, int warps) {
+    const uint32_t n = ctx->n, nc = ctx->nc;
+    const size_t nr = (size_t)n * R;
+    ENSURE(ctx->bE, nr * 12);
+    ENSURE(ctx->bdirect, nr * 16);
+    ENSURE(ctx->brad, nr * 16);
+    ENSURE(ctx->birr, nr * 16);
+    ENSURE(ctx->bcrad, (size_t)nc * R * 16);
+    ENSURE(ctx->bdone, (size_t)R * 4);
+    ENSURE(ctx->biters, (size_t)R * 4);
+    ENSURE(ctx->bres, (size_t)R * 4);
+    ENSURE(ctx->blast, (size_t)R * 4);
+    if (E) {
+        CK(cudaMemcpyAsync(ctx->bE.p, E, nr * 12, cudaMemcpyHostToDevice, ctx->st));
+        ctx->bE_n = n;
+        ctx->bE_R = R;
+    } else if (ctx->bE_n != n || ctx->bE_R != R) {
+        return fail(ctx, IFX_ERR_INVALID, "no resident right-hand sides of this shape: pass E");
+    }
+    ctx->launches += (uint64_t)launch_batch_init(ctx->st, (const float*)ctx->bE.p, n, R, (float4*)ctx->bdirect.p,
+                                                 (float4*)ctx->brad.p, (float4*)ctx->birr.p);
+    for (DBuf* b : {&ctx->bdone, &ctx->biters, &ctx->bres, &ctx->blast})
+        CK(cudaMemsetAsync(b->p, 0, (size_t)R * 4, ctx->st));
+    std::vector<uint32_t> done(R);
+    const uint32_t kBatch = 16;
+    for (uint32_t it = 0; it < max_bounces;) {
+        uint32_t end = it + kBatch < max_bounces ? it + kBatch : max_bounces;
+        for (; it < end; ++it)
+            ctx->launches += (uint64_t)launch_batched_bounce(
+                ctx->st, n, R, (const float4*)ctx->sp.p, (const float4*)ctx->salb.p, (const float4*)ctx->bdirect.p,
+                (float4*)ctx->birr.p, (float4*)ctx->brad.p, (const float4*)ctx->cp.p, (const uint2*)ctx->crange.p,
+                (const uint32_t*)ctx->members.p, nc, (const uint32_t*)ctx->starts.p, (const uint32_t*)ctx->idx.p,
+                (const float*)ctx->w.p, (float4*)ctx->bcrad.p, (uint32_t*)ctx->bdone.p, (uint32_t*)ctx->biters.p,
+                (uint32_t*)ctx->bres.p, (uint32_t*)ctx->blast.p, it, warps);
+        CKL();
+        CK(cudaMemcpyAsync(done.data(), ctx->bdone.p, (size_t)R * 4, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        bool all = true;
+        for (uint32_t v : done) all = all && v;
+        if (all) break;
+    }
+    return IFX_OK;
+}
+
+extern "C" int ifx_solve_batched(ifx_ctx* ctx, uint32_t R, const float* E, uint32_t max_bounces, float* rad_out,
+                                 float* irr_out, uint32_t* iterations, float* residual) {
+    if (!ctx || R == 0) return fail(ctx, IFX_ERR_INVALID, "bad argument");
+    if (!ctx->has_transfer || ctx->nc == 0) return fail(ctx, IFX_ERR_INVALID, "no transfer");
+    CK(cudaSetDevice(ctx->device));
+    const uint32_t n = ctx->n;
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    int r = batched_run(ctx, R, E, max_bounces, ctx->spmm_warps);
+    if (r) return r;
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    const size_t nr = (size_t)n * R;
+    for (int k = 0; k < 2; ++k) {
+        float* dst = k == 0 ? rad_out : irr_out;
+        if (!dst) continue;
+        ENSURE(ctx->bunpack, nr * 12);
+        ctx->launches += (uint64_t)launch_batch_unpack(ctx->st, (const float4*)(k == 0 ? ctx->brad.p : ctx->birr.p), n,
+                                                       R, (float*)ctx->bunpack.p);
+        CK(cudaMemcpyAsync(dst, ctx->bunpack.p, nr * 12, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    if (iterations) CK(cudaMemcpyAsync(iterations, ctx->biters.p, (size_t)R * 4, cudaMemcpyDeviceToHost, ctx->st));
+    if (residual) CK(cudaMemcpyAsync(residual, ctx->blast.p, (size_t)R * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaEventElapsedTime(&ctx->stats.ms_solve, ctx->ev0, ctx->ev1));
+    return IFX_OK;
+}
+
+extern "C" int ifx_autotune_batched(ifx_ctx* ctx, uint32_t R, const float* E, int* best) {
+    if (!ctx || !E || R == 0) return fail(ctx, IFX_ERR_INVALID, "bad argument");
+    if (!ctx->has_transfer || ctx->nc == 0) return fail(ctx, IFX_ERR_INVALID, "no transfer");
+    CK(cudaSetDevice(ctx->device));
+    float best_ms = 3.4e38f;
+    int best_w = ctx->spmm_warps;
+    for (int warps : {2, 4, 8, 16}) {
+        float total = 0.0f;
+        for (int rep = 0; rep < 3; ++rep) {
+            CK(cudaEventRecord(ctx->tm0, ctx->st));
+            int r = batched_run(ctx, R, E, 4, warps);
+            if (r) return r;
+            CK(cudaEventRecord(ctx->tm1, ctx->st));
+            CK(cudaEventSynchronize(ctx->tm1));
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, ctx->tm0, ctx->tm1));
+            if (rep > 0) total += ms;
+        }
+        if (total < best_ms) {
+            best_ms = total;
+            best_w = warps;
+        }
+    }
+    ctx->spmm_warps = best_w;
+    if (best) *best = best_w;
     return IFX_OK;
 }
 

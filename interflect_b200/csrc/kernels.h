@@ -103,6 +103,16 @@ void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const floa
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
                          const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches);
 
+// ---- batched relighting (solve.rs:47-108 over R right-hand sides) ----
+int launch_batch_init(cudaStream_t st, const float* E, uint32_t n, uint32_t R, float4* direct, float4* rad,
+                      float4* irr);
+int launch_batch_unpack(cudaStream_t st, const float4* x, uint32_t n, uint32_t R, float* out);
+int launch_batched_bounce(cudaStream_t st, uint32_t n, uint32_t R, const float4* sp, const float4* albedo,
+                          const float4* direct, float4* irr, float4* rad, const float4* cp, const uint2* crange,
+                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
+                          const float* w, float4* crad, uint32_t* done, uint32_t* iterations, uint32_t* res_bits,
+                          uint32_t* last_res, uint32_t it, int rows_per_block_warps);
+
 // ---- grid + shade (surfel.rs:71-114, main.rs:229-367, film.rs:51-61) ----
 void launch_grid_keys(cudaStream_t st, const float4* p, uint32_t n, GridParams g, unsigned long long* keys);
 void launch_grid_starts(cudaStream_t st, const unsigned long long* sorted, uint32_t n, uint32_t ncells,
