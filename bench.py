@@ -86,7 +86,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (OSError, FileNotFoundError):
@@ -186,6 +186,9 @@ def run_ours(args, world, rank, local) -> dict | None:
     with open(os.path.join(ROOT, scene_path)) as f:
         src = f.read()
     scene = ifx.parse(src)
+    if args.film:
+        fw, fh = (int(v) for v in args.film.lower().split("x"))
+        scene.set_cfg(width=fw, height=fh)
     cfg = scene.cfg
     ctx = ifx.Context(local)
     ctx.upload(scene)
@@ -455,12 +458,13 @@ def run_reference(args, world, rank) -> dict | None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2_product", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rows", type=float, default=1.0, help="fraction of film rows the CPU legs shade")
+    ap.add_argument("--film", default=None, help="WxH film override for small profiling cases (e.g. 640x360)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256) k_agg_batched(const float4* rad, const fl
 // solve.rs:76-102 for every rhs: blockIdx.y picks 32 rhs, warps stride over
 // rows; a lane keeps its rhs for the whole kernel and reduces its residual
 // to one integer atomicMax at the end.
-__global__ void __launch_bounds__(256) k_spmm(const float4* direct, const float4* albedo, float4* irr, float4* rad,
+__global__ void __launch_bounds__(512) k_spmm(const float4* direct, const float4* albedo, float4* irr, float4* rad,
                                                uint32_t n, uint32_t R, const uint32_t* starts, const uint32_t* idx,
                                                const float* w, const float4* crad, const uint32_t* done,
                                                uint32_t* res_bits) {
