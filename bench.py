@@ -42,7 +42,12 @@ WORKLOADS = {
     "c4_batch": ("interflect_b200/scenes/c1_cornell.rad",
                  "256 relighting right-hand sides (1-4 surfels-as-lights, intensity U[1,50]) on the Cornell "
                  "transfer, one CSR SpMM solve, 12 bounces max"),
+    "c5_diff": ("interflect_b200/scenes/c5_cornell_fill.rad",
+                "Cornell box 512x512 with a second (fill) light, 20k surfels, 12 fixed bounces; L2 loss against a "
+                "target rendered from per-surfel albedo + N(0,0.05) clamped to [0.05,0.95]; gradient w.r.t. "
+                "per-surfel albedo and both light emissions"),
 }
+DIFF_METRIC = "albedo+emission gradient ms (differentiable forward + adjoint) vs one forward frame"
 BATCH_METRIC = "relighting solves per second (256 right-hand sides on one transfer matrix)"
 METRIC = "SDF evaluations per second, one full frame (transfer + light + solve + grid + shade)"
 # Kernels with per-launch CUDA-event times and work counters (the ray-marching
@@ -376,6 +381,83 @@ def run_batch(args, world, rank, local) -> dict | None:
     }
 
 
+def run_diff(args, world, rank, local) -> dict | None:
+    """Differentiation: one gradient step (the frame for the current albedo
+    and emission, the loss gradient on the host, the adjoint) against one
+    forward frame of the same scene through the plain pipeline."""
+    import numpy as np
+    import interflect_b200 as ifx
+    scene_path, desc = WORKLOADS[args.workload]
+    with open(os.path.join(ROOT, scene_path)) as f:
+        src = f.read()
+    scene = ifx.parse(src)
+    cfg = scene.cfg
+    ctx = ifx.Context(local)
+    ctx.upload(scene)
+    placed = ctx.generate(cfg.surfels)
+    flusher = L2Flusher(local)
+    # One forward frame as the renderer makes it (transfer + light + solve +
+    # grid + shade), CUDA-event timed.
+    for _ in range(args.warmup):
+        frame(ctx, cfg)
+    fwd = []
+    for _ in range(args.steps):
+        flusher.flush()
+        ctx.timer_start()
+        info, _, _, _ = frame(ctx, cfg)
+        fwd.append(ctx.timer_stop())
+    # Differentiable frame: geometry, visibility and the transposes once.
+    K = cfg.bounces
+    dinfo = ctx.diff_setup(cfg.width, cfg.height, K)
+    surf = ctx.surfels()
+    rng = np.random.default_rng(2026)
+    rho0 = surf["albedo"]
+    rho_t = np.clip(rho0 + rng.normal(0.0, 0.05, rho0.shape), 0.05, 0.95).astype(np.float32)
+    emit0 = ctx.light_emission()
+    target = ctx.diff_forward(rho_t, emit0)
+    for _ in range(args.warmup):
+        img = ctx.diff_forward(rho0, emit0)
+        ctx.diff_backward(2.0 * (img - target))
+    barrier(world)
+    launches0 = ctx.stats()["kernel_launches"]
+    dev_f, dev_b, e2e = [], [], []
+    for _ in range(args.steps):
+        flusher.flush()
+        ctx.timer_start()
+        img = ctx.diff_forward(rho0, emit0)
+        g_img = 2.0 * (img - target)
+        g_rho, g_e = ctx.diff_backward(g_img)
+        e2e.append(ctx.timer_stop())
+        st = ctx.stats()
+        dev_f.append(st["ms_diff_forward"])
+        dev_b.append(st["ms_diff_backward"])
+    launches = ctx.stats()["kernel_launches"] - launches0
+    (grad_max, fwd_max, e2e_max), _ = allreduce_max_sum(
+        [statistics.median([f + b for f, b in zip(dev_f, dev_b)]), statistics.median(fwd), statistics.median(e2e)],
+        [0.0], world)
+    if rank != 0:
+        return None
+    loss = float(((img - target) ** 2).sum())
+    return {
+        "metric": DIFF_METRIC, "value": grad_max, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": grad_max, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "scene": scene_path, "description": desc, "film": [cfg.width, cfg.height],
+                   "surfels_placed": placed, "clusters": info.clusters, "links": info.links, "bounces": K,
+                   "gather_entries": dinfo["gather_entries"], "lights": dinfo["lights"],
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "forward_frame_ms": fwd_max,
+        "gradient_over_forward": grad_max / fwd_max,
+        "gradient_device_ms": {"forward": statistics.median(dev_f), "adjoint": statistics.median(dev_b)},
+        "setup_ms": dinfo["ms_setup"],
+        "loss": loss, "grad_rho_norm": float(np.linalg.norm(g_rho)), "grad_emit": g_e.tolist(),
+        "e2e": {"value": e2e_max, "unit": "ms", "h2d_bytes_per_step": int(rho0.nbytes + emit0.nbytes + g_img.nbytes),
+                "d2h_bytes_per_step": int(img.nbytes + g_rho.nbytes + g_e.nbytes),
+                "includes": "albedo+emission upload, frame download, host loss gradient, adjoint, gradient download"},
+        "gpu_launches": int(launches),
+    }
+
+
 def cpu_frame(src, surf, cfg, threads, rows_frac=1.0):
     """One frame of the oracle (the reference algorithm on the CPU) on the
     given surfels; shading restricted to the first rows_frac of the rows."""
@@ -473,6 +555,8 @@ def main():
             line = run_reference(args, world, rank)
         elif args.workload == "c4_batch":
             line = run_batch(args, world, rank, local)
+        elif args.workload == "c5_diff":
+            line = run_diff(args, world, rank, local)
         else:
             line = run_ours(args, world, rank, local)
         if line is not None:

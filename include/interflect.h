@@ -106,6 +106,8 @@ typedef struct ifx_stats {
      * shadow cones of the camera hits, mirror rays, shadow cones of the
      * mirror hits, and the rest (setup, mirror setup, compose + encode). */
     float ms_primary, ms_shadow, ms_reflect, ms_shadow2, ms_shade_other;
+    /* CUDA-event times of the last differentiable forward and backward. */
+    float ms_diff_forward, ms_diff_backward;
 } ifx_stats;
 
 /* Kernels, for work accounting (ifx_get_work). */
@@ -284,6 +286,54 @@ int ifx_grid_build(ifx_ctx* ctx, float radius);
  * `evals` receives the SDF evaluation count (nullable). */
 int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
                      float* out_linear, uint8_t* out_srgb, uint64_t* evals);
+
+/* --------------------------------------------------- differentiation --- */
+/* Gradients of an image loss with respect to per-surfel albedo and per-light
+ * emission, geometry and visibility held fixed. None of this has a
+ * counterpart in the reference, whose surfel albedo is always the material's
+ * diffuse albedo (surfel.rs:244) and whose solve stops on its residual. */
+
+/* Per-surfel albedo override: rho (host, n x 3) replaces every surfel's
+ * albedo, the value solve::light_surfels and solve::solve read
+ * (solve.rs:33, :80). The transfer and grid stay valid. */
+int ifx_surfels_set_albedo(ifx_ctx* ctx, const float* rho);
+/* Per-light emission (host, nl x 3; quad lights in scene order, then sphere
+ * lights) of the uploaded scene. The transfer, surfels and grid stay valid. */
+int ifx_lights_set_emission(ifx_ctx* ctx, uint32_t nl, const float* emit);
+int ifx_lights_get_emission(ifx_ctx* ctx, uint32_t nl, float* emit);
+
+typedef struct ifx_diff_info {
+    uint64_t surfels, lights, pixels;
+    uint64_t gather_entries; /* (pixel, surfel) pairs of the frame's gathers */
+    uint64_t links;          /* entries of the transposed transfer */
+    uint32_t bounces;        /* the fixed bounce count K */
+    float ms_setup;
+} ifx_diff_info;
+
+/* Prepares the differentiable frame of camera `cam` (NULL: the scene's) at
+ * w x h, beauty mode, with exactly `bounces` Jacobi bounces (no residual
+ * exit). Needs an uploaded scene, surfels and a transfer. Traces the frame
+ * once (light factors of every surfel, the frame's hits, form factors and
+ * visibilities), builds the gather grid, the per-pixel emission
+ * coefficients, and the transposed gather and transfer operators. Any later
+ * call that rebuilds the transfer or grid, uploads a scene or surfels, or
+ * renders a frame ends the prepared state. */
+int ifx_diff_setup(ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, uint32_t h, uint32_t bounces,
+                   ifx_diff_info* out);
+/* The prepared frame for albedo rho (n x 3) and emission emit (nl x 3), both
+ * nullable (keep the current values): solve::light_surfels' result from the
+ * stored light factors, `bounces` Jacobi bounces with their irradiance kept
+ * for the adjoint, and the frame re-composed from the stored hits. The image
+ * (w*h*3 linear f32, nullable) is bit-identical to ifx_render_frame's after
+ * ifx_light_surfels, a fixed-bounce solve and ifx_grid_build with the same
+ * albedo and emission. */
+int ifx_diff_forward(ifx_ctx* ctx, const float* rho, const float* emit, float* image);
+/* Reverse mode of the last ifx_diff_forward for dL/dimage (w*h*3):
+ * dL/drho (n x 3) and dL/demit (nl x 3), both nullable. The adjoint runs the
+ * bounces backwards on the GPU-built transposes, (I - diag(rho) F A)^T
+ * truncated to the same K bounces, in a fixed summation order (bit-identical
+ * across runs). */
+int ifx_diff_backward(ifx_ctx* ctx, const float* grad_image, float* grad_rho, float* grad_emit);
 
 #ifdef __cplusplus
 }

@@ -44,6 +44,8 @@ EXPORTS = (
     "ifx_transfer_upload", "ifx_light_surfels", "ifx_solve", "ifx_grid_build", "ifx_render_frame",
     "ifx_set_work_counting", "ifx_reset_work", "ifx_get_work", "ifx_timer_start", "ifx_timer_stop",
     "ifx_solve_noalloc", "ifx_surfels_set_emission", "ifx_solve_batched", "ifx_autotune_batched",
+    "ifx_surfels_set_albedo", "ifx_lights_set_emission", "ifx_lights_get_emission", "ifx_diff_setup",
+    "ifx_diff_forward", "ifx_diff_backward",
 )
 NOALLOC_MAX_CLUSTERS = 16384
 KERNELS = {"visibility": 0, "closure": 1, "light": 2, "primary": 3, "shadow": 4, "reflect": 5, "shadow2": 6,
@@ -93,7 +95,13 @@ class _Stats(C.Structure):
                 ("ms_solve", C.c_float), ("ms_grid", C.c_float), ("ms_shade", C.c_float),
                 ("ms_visibility", C.c_float), ("ms_closure", C.c_float), ("ms_primary", C.c_float),
                 ("ms_shadow", C.c_float), ("ms_reflect", C.c_float), ("ms_shadow2", C.c_float),
-                ("ms_shade_other", C.c_float)]
+                ("ms_shade_other", C.c_float), ("ms_diff_forward", C.c_float), ("ms_diff_backward", C.c_float)]
+
+
+class _DiffInfo(C.Structure):
+    _fields_ = [("surfels", C.c_uint64), ("lights", C.c_uint64), ("pixels", C.c_uint64),
+                ("gather_entries", C.c_uint64), ("links", C.c_uint64), ("bounces", C.c_uint32),
+                ("ms_setup", C.c_float)]
 
 
 _lib_handle = None
@@ -143,6 +151,12 @@ def lib() -> C.CDLL:
         "ifx_surfels_set_emission": (I, [P, P]),
         "ifx_solve_batched": (I, [P, U32, P, U32, P, P, P, P]),
         "ifx_autotune_batched": (I, [P, U32, P, C.POINTER(I)]),
+        "ifx_surfels_set_albedo": (I, [P, P]),
+        "ifx_lights_set_emission": (I, [P, U32, P]),
+        "ifx_lights_get_emission": (I, [P, U32, P]),
+        "ifx_diff_setup": (I, [P, C.POINTER(_Camera), U32, U32, U32, C.POINTER(_DiffInfo)]),
+        "ifx_diff_forward": (I, [P, P, P, P]),
+        "ifx_diff_backward": (I, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -443,6 +457,59 @@ class Context:
         s = _Stats()
         lib().ifx_get_stats(self._h, C.byref(s))
         return {f: getattr(s, f) for f, _ in _Stats._fields_}
+
+    # -- differentiation ----------------------------------------------------
+    @property
+    def n_lights(self) -> int:
+        i = self.scene.info if self.scene is not None else None
+        return 0 if i is None else i.lights + i.sphere_lights
+
+    def set_albedo(self, rho) -> None:
+        """Per-surfel albedo override (n x 3)."""
+        rho = np.ascontiguousarray(rho, np.float32).reshape(-1, 3)
+        if len(rho) != self.n_surfels:
+            raise ValueError(f"albedo has {len(rho)} rows for {self.n_surfels} surfels")
+        self._check(lib().ifx_surfels_set_albedo(self._h, _ptr(rho)), "set_albedo")
+
+    def set_light_emission(self, emit) -> None:
+        """Per-light emission (nl x 3: quad lights, then sphere lights)."""
+        emit = np.ascontiguousarray(emit, np.float32).reshape(-1, 3)
+        self._check(lib().ifx_lights_set_emission(self._h, len(emit), _ptr(emit)), "set_light_emission")
+
+    def light_emission(self) -> np.ndarray:
+        out = np.zeros((self.n_lights, 3), np.float32)
+        self._check(lib().ifx_lights_get_emission(self._h, len(out), _ptr(out)), "light_emission")
+        return out
+
+    def diff_setup(self, width: int, height: int, bounces: int, cam=None) -> dict:
+        """Prepares the differentiable beauty frame (fixed bounce count)."""
+        i = _DiffInfo()
+        self._check(lib().ifx_diff_setup(self._h, C.byref(cam) if cam is not None else None, width, height,
+                                         bounces, C.byref(i)), "diff_setup")
+        self._diff_shape = (height, width)
+        return {f: getattr(i, f) for f, _ in _DiffInfo._fields_}
+
+    def diff_forward(self, rho=None, emit=None) -> np.ndarray:
+        """The prepared frame (H x W x 3 linear f32) for albedo rho and emission emit."""
+        if rho is not None:
+            rho = np.ascontiguousarray(rho, np.float32).reshape(-1, 3)
+            if len(rho) != self.n_surfels:
+                raise ValueError(f"albedo has {len(rho)} rows for {self.n_surfels} surfels")
+        if emit is not None:
+            emit = np.ascontiguousarray(emit, np.float32).reshape(-1, 3)
+            if len(emit) != self.n_lights:
+                raise ValueError(f"emission has {len(emit)} rows for {self.n_lights} lights")
+        img = np.zeros(self._diff_shape + (3,), np.float32)
+        self._check(lib().ifx_diff_forward(self._h, _ptr(rho), _ptr(emit), _ptr(img)), "diff_forward")
+        return img
+
+    def diff_backward(self, grad_image) -> tuple[np.ndarray, np.ndarray]:
+        """(dL/drho n x 3, dL/demit nl x 3) for dL/dimage of the last diff_forward."""
+        g = np.ascontiguousarray(grad_image, np.float32).reshape(self._diff_shape + (3,))
+        gr = np.zeros((self.n_surfels, 3), np.float32)
+        ge = np.zeros((self.n_lights, 3), np.float32)
+        self._check(lib().ifx_diff_backward(self._h, _ptr(g), _ptr(gr), _ptr(ge)), "diff_backward")
+        return gr, ge
 
     # -- measurement ----------------------------------------------------------
     def set_work_counting(self, on: bool) -> None:

@@ -25,7 +25,8 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "lib", "libinterflect_b200.so")
 CLI = os.path.join(HERE, "bin", "interflect")
 
-CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "k_batch.cu", "capi.cu", "noalloc.cu"]
+CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "k_batch.cu", "k_diff.cu", "capi.cu",
+              "noalloc.cu"]
 CPP_SOURCES = ["scene_host.cpp"]
 HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh", "flop_model.h"]
 

@@ -86,6 +86,23 @@ struct ifx_ctx {
     // film
     DBuf film, out8;
 
+    // lights: current emission per light (float4), for the relight and adjoint
+    DBuf lemit;
+    uint32_t nl = 0;
+
+    // differentiation: the prepared frame and the transposed operators
+    bool diff_ready = false;
+    uint32_t diff_K = 0;
+    uint64_t diff_entries = 0, diff_links = 0;
+    ShadeParams diff_P{};
+    DBuf dterms;                                    // n x nl light factors
+    DBuf dpix, dcnt, doff;                          // per pixel: emission coefficients, gather counts, offsets
+    DBuf dkey, dkey_alt, dperm, dperm_alt, draw;    // gather entries before / during the sort
+    DBuf gent, gtstarts;                            // G^T: sorted entries, surfel row starts
+    DBuf lrows, fkey_alt, ft, ftstarts, cid;        // F^T and cluster membership
+    DBuf hist;                                      // irr_1 .. irr_{K-1}
+    DBuf dg, h_t, yv, ebar, rhobar, epart, eout, d3; // backward work
+
     // scratch
     DBuf cub_tmp, small;  // small: 8 x u64 counters / results
     DBuf gen_cand;
@@ -185,6 +202,14 @@ static int cub_call(ifx_ctx* ctx, F f) {
         int r_ = cub_call(ctx, expr);         \
         if (r_ != IFX_OK) return r_;          \
     } while (0)
+
+// Emission of every light, quad lights then sphere lights.
+static std::vector<float4> light_emissions(const HScene& s) {
+    std::vector<float4> v;
+    for (const HQuadLight& l : s.lights) v.push_back(make_float4(l.emit.x, l.emit.y, l.emit.z, 0.0f));
+    for (const HSphereLight& l : s.sphere_lights) v.push_back(make_float4(l.emit.x, l.emit.y, l.emit.z, 0.0f));
+    return v;
+}
 
 static void copy_err(const std::string& m, char* err, size_t errlen) {
     if (!err || errlen == 0) return;
@@ -336,7 +361,11 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->w, &ctx->cluster_rad, &ctx->ctl, &ctx->gkeys, &ctx->gkeys_alt, &ctx->gstarts, &ctx->gp,
                     &ctx->gn, &ctx->girr, &ctx->gitems, &ctx->film, &ctx->out8, &ctx->cub_tmp, &ctx->small,
                     &ctx->gen_cand, &ctx->work, &ctx->bE, &ctx->bdirect, &ctx->brad, &ctx->birr, &ctx->bcrad,
-                    &ctx->bdone, &ctx->biters, &ctx->bres, &ctx->blast, &ctx->bunpack};
+                    &ctx->bdone, &ctx->biters, &ctx->bres, &ctx->blast, &ctx->bunpack, &ctx->lemit,
+                    &ctx->dterms, &ctx->dpix, &ctx->dcnt, &ctx->doff, &ctx->dkey, &ctx->dkey_alt, &ctx->dperm,
+                    &ctx->dperm_alt, &ctx->draw, &ctx->gent, &ctx->gtstarts, &ctx->lrows, &ctx->fkey_alt,
+                    &ctx->ft, &ctx->ftstarts, &ctx->cid, &ctx->hist, &ctx->dg, &ctx->h_t, &ctx->yv, &ctx->ebar,
+                    &ctx->rhobar, &ctx->epart, &ctx->eout, &ctx->d3};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -421,7 +450,12 @@ extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     std::vector<uint8_t> blob = flatten_scene(s);
     ENSURE(ctx->blob, blob.size());
     CK(cudaMemcpyAsync(ctx->blob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->st));
+    std::vector<float4> le = light_emissions(s);
+    ENSURE(ctx->lemit, le.size() * 16);
+    if (!le.empty()) CK(cudaMemcpyAsync(ctx->lemit.p, le.data(), le.size() * 16, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    ctx->nl = (uint32_t)le.size();
+    ctx->diff_ready = false;
     ctx->scene = s;
     ctx->blobref.ptr = (const uint8_t*)ctx->blob.p;
     ctx->blobref.bytes = (uint32_t)blob.size();
@@ -431,6 +465,7 @@ extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     ctx->has_scene = true;
     ctx->has_transfer = false;
     ctx->has_grid = false;
+    ctx->diff_ready = false;
     return IFX_OK;
 }
 
@@ -475,6 +510,7 @@ extern "C" int ifx_surfels_upload(ifx_ctx* ctx, uint64_t n, const float* p, cons
     ctx->n = (uint32_t)n;
     ctx->has_transfer = false;
     ctx->has_grid = false;
+    ctx->diff_ready = false;
     return IFX_OK;
 }
 
@@ -609,6 +645,7 @@ extern "C" int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* pla
     ctx->n = n;
     ctx->has_transfer = false;
     ctx->has_grid = false;
+    ctx->diff_ready = false;
     if (placed) *placed = n;
     return IFX_OK;
 }
@@ -789,6 +826,7 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     ctx->links = links;
     ctx->has_transfer = true;
     ctx->has_grid = false;
+    ctx->diff_ready = false;
     if (out) {
         float mean;
         memcpy(&mean, &hs[0], 4);
@@ -878,6 +916,7 @@ extern "C" int ifx_transfer_upload(ifx_ctx* ctx, const uint32_t* starts, uint64_
     CK(cudaStreamSynchronize(ctx->st));
     ctx->links = links;
     ctx->has_transfer = true;
+    ctx->diff_ready = false;
     return IFX_OK;
 }
 
@@ -1121,11 +1160,14 @@ extern "C" int ifx_grid_build(ifx_ctx* ctx, float radius) {
     ctx->grid = g;
     ctx->ncells = ncells;
     ctx->has_grid = true;
+    ctx->diff_ready = false;
     return IFX_OK;
 }
 
-extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
-                                float* out_linear, uint8_t* out_srgb, uint64_t* evals) {
+// keep_film: the linear film stays in device memory (ctx->film) even when no
+// host copy is asked for; saved (nullable) receives the launch parameters.
+static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
+                       float* out_linear, uint8_t* out_srgb, uint64_t* evals, bool keep_film, ShadeParams* saved) {
     if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
     if (mode < 0 || mode > 5) return fail(ctx, IFX_ERR_INVALID, "unknown mode");
     if (w == 0 || h == 0 || w > 16384u || h > 16384u || (uint64_t)w * h > 40000000ull)
@@ -1160,7 +1202,7 @@ extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, u
     P.tonemap = mode <= IFX_MODE_INDIRECT ? 1 : 0;
     P.srgb_t = (const float*)ctx->srgb_t.p;
     size_t px = (size_t)w * h;
-    if (out_linear) {
+    if (out_linear || keep_film) {
         ENSURE(ctx->film, px * 12);
         P.film = (float*)ctx->film.p;
     }
@@ -1222,5 +1264,262 @@ extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, u
     ctx->stats.ms_shadow2 = g[3];
     ctx->stats.ms_shade_other = g[4] + g[5] + g[6];
     if (evals) *evals = e;
+    if (saved) *saved = P;
+    return IFX_OK;
+}
+
+extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
+                                float* out_linear, uint8_t* out_srgb, uint64_t* evals) {
+    if (ctx) ctx->diff_ready = false;  // the wavefront buffers are about to be overwritten
+    return render_impl(ctx, cam, mode, w, h, exposure, out_linear, out_srgb, evals, false, nullptr);
+}
+
+// ------------------------------------------------------ differentiation ---
+extern "C" int ifx_surfels_set_albedo(ifx_ctx* ctx, const float* rho) {
+    if (!ctx || (!rho && ctx->n)) return fail(ctx, IFX_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    const uint32_t n = ctx->n;
+    std::vector<float4> h(n);
+    for (uint32_t i = 0; i < n; ++i) h[i] = make_float4(rho[3 * i], rho[3 * i + 1], rho[3 * i + 2], 0.0f);
+    if (n) CK(cudaMemcpyAsync(ctx->salb.p, h.data(), (size_t)n * 16, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return IFX_OK;
+}
+
+extern "C" int ifx_lights_set_emission(ifx_ctx* ctx, uint32_t nl, const float* emit) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (nl != ctx->nl || (nl && !emit)) return fail(ctx, IFX_ERR_INVALID, "light count does not match the scene");
+    CK(cudaSetDevice(ctx->device));
+    HScene& s = ctx->scene;
+    uint32_t k = 0;
+    for (HQuadLight& l : s.lights) {
+        l.emit = F3{emit[3 * k], emit[3 * k + 1], emit[3 * k + 2]};
+        ++k;
+    }
+    for (HSphereLight& l : s.sphere_lights) {
+        l.emit = F3{emit[3 * k], emit[3 * k + 1], emit[3 * k + 2]};
+        ++k;
+    }
+    // The program blob carries the emissions the shading kernels read; the
+    // flattened layout is otherwise unchanged, so the device copy is
+    // replaced in place.
+    std::vector<uint8_t> blob = flatten_scene(s);
+    if (blob.size() != ctx->blobref.bytes) return fail(ctx, IFX_ERR_INVALID, "scene layout changed");
+    std::vector<float4> le = light_emissions(s);
+    CK(cudaMemcpyAsync(ctx->blob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->st));
+    if (nl) CK(cudaMemcpyAsync(ctx->lemit.p, le.data(), (size_t)nl * 16, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return IFX_OK;
+}
+
+extern "C" int ifx_lights_get_emission(ifx_ctx* ctx, uint32_t nl, float* emit) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (nl != ctx->nl || (nl && !emit)) return fail(ctx, IFX_ERR_INVALID, "light count does not match the scene");
+    std::vector<float4> le = light_emissions(ctx->scene);
+    for (uint32_t l = 0; l < nl; ++l) {
+        emit[3 * l] = le[l].x;
+        emit[3 * l + 1] = le[l].y;
+        emit[3 * l + 2] = le[l].z;
+    }
+    return IFX_OK;
+}
+
+extern "C" int ifx_diff_setup(ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, uint32_t h, uint32_t bounces,
+                              ifx_diff_info* out) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (!ctx->has_transfer || ctx->nc == 0 || ctx->n == 0) return fail(ctx, IFX_ERR_INVALID, "no transfer");
+    if (bounces == 0 || bounces > 256) return fail(ctx, IFX_ERR_LIMIT, "bounces out of range (1..256)");
+    CK(cudaSetDevice(ctx->device));
+    ctx->diff_ready = false;
+    const uint32_t n = ctx->n, nc = ctx->nc, nl = ctx->nl;
+    const auto t_start = std::chrono::steady_clock::now();
+    // 1. Each surfel's light factors (with direct = rad = E as a side effect).
+    ENSURE(ctx->dterms, (size_t)n * (nl ? nl : 1) * 4);
+    unsigned long long* small = (unsigned long long*)ctx->small.p;
+    launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), n, small, (uint32_t*)ctx->status.p, nullptr,
+                         (float*)ctx->dterms.p);
+    ctx->launches++;
+    CKL();
+    int r = check_status(ctx);
+    if (r) return r;
+    // 2. Gather grid and 3. the frame's hits, form factors and visibilities.
+    if ((r = ifx_grid_build(ctx, 0.0f))) return r;
+    ShadeParams P{};
+    if ((r = render_impl(ctx, cam, IFX_MODE_BEAUTY, w, h, 1.0f, nullptr, nullptr, nullptr, true, &P))) return r;
+    if (!P.has_gi) return fail(ctx, IFX_ERR_INVALID, "no gather grid");
+    P.counts = nullptr;
+    P.recompose = 1;
+    const uint32_t px = w * h;
+    // 4. Per-pixel emission coefficients and gather entries (count, scan, fill).
+    ENSURE(ctx->dpix, (size_t)px * (nl ? nl : 1) * 16);
+    ENSURE(ctx->dcnt, ((size_t)px + 1) * 4);
+    ENSURE(ctx->doff, ((size_t)px + 1) * 4);
+    ctx->launches += (uint64_t)launch_diff_pixels(ctx->st, P, 0, (float4*)ctx->dpix.p, (uint32_t*)ctx->dcnt.p,
+                                                  nullptr, nullptr, nullptr, nullptr);
+    CKL();
+    CK(cudaMemsetAsync((uint32_t*)ctx->dcnt.p + px, 0, 4, ctx->st));
+    uint32_t* dcnt = (uint32_t*)ctx->dcnt.p;
+    uint32_t* doff = (uint32_t*)ctx->doff.p;
+    CUB([&](void* t, size_t& b) { return cub::DeviceScan::ExclusiveSum(t, b, dcnt, doff, (int)px + 1, ctx->st); });
+    uint32_t E = 0;
+    CK(cudaMemcpyAsync(&E, doff + px, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ENSURE(ctx->dkey, (size_t)E * 4);
+    ENSURE(ctx->dkey_alt, (size_t)E * 4);
+    ENSURE(ctx->dperm, (size_t)E * 4);
+    ENSURE(ctx->dperm_alt, (size_t)E * 4);
+    ENSURE(ctx->draw, (size_t)E * 16);
+    ENSURE(ctx->gent, (size_t)E * 16);
+    ENSURE(ctx->gtstarts, ((size_t)n + 1) * 4);
+    if (E) {
+        ctx->launches += (uint64_t)launch_diff_pixels(ctx->st, P, 1, (float4*)ctx->dpix.p, dcnt, doff,
+                                                      (const uint32_t*)ctx->gitems.p, (uint32_t*)ctx->dkey.p,
+                                                      (float4*)ctx->draw.p);
+        ctx->launches += (uint64_t)launch_iota(ctx->st, (uint32_t*)ctx->dperm.p, E);
+        CKL();
+        int end_bit = 1;
+        while (end_bit < 32 && (1u << end_bit) < n) ++end_bit;
+        uint32_t *kin = (uint32_t*)ctx->dkey.p, *kout = (uint32_t*)ctx->dkey_alt.p;
+        uint32_t *vin = (uint32_t*)ctx->dperm.p, *vout = (uint32_t*)ctx->dperm_alt.p;
+        CUB([&](void* t, size_t& b) {
+            return cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int)E, 0, end_bit, ctx->st);
+        });
+        ctx->launches += (uint64_t)launch_permute_entries(ctx->st, vout, (const float4*)ctx->draw.p, E,
+                                                          (float4*)ctx->gent.p);
+        ctx->launches += (uint64_t)launch_csr_starts(ctx->st, kout, E, n, (uint32_t*)ctx->gtstarts.p);
+    } else {
+        CK(cudaMemsetAsync(ctx->gtstarts.p, 0, ((size_t)n + 1) * 4, ctx->st));
+    }
+    CKL();
+    // 5. F^T: the transfer's entries stably sorted by cluster.
+    const uint32_t L = (uint32_t)ctx->links;
+    ENSURE(ctx->lrows, (size_t)L * 4);
+    ENSURE(ctx->fkey_alt, (size_t)L * 4);
+    ENSURE(ctx->dperm, (size_t)L * 4);
+    ENSURE(ctx->dperm_alt, (size_t)L * 4);
+    ENSURE(ctx->ft, (size_t)L * 8);
+    ENSURE(ctx->ftstarts, ((size_t)nc + 1) * 4);
+    ctx->launches += (uint64_t)launch_link_rows(ctx->st, (const uint32_t*)ctx->starts.p, n, (uint32_t*)ctx->lrows.p);
+    if (L) {
+        ctx->launches += (uint64_t)launch_iota(ctx->st, (uint32_t*)ctx->dperm.p, L);
+        CKL();
+        int end_bit = 1;
+        while (end_bit < 32 && (1u << end_bit) < nc) ++end_bit;
+        const uint32_t* kin = (const uint32_t*)ctx->idx.p;
+        uint32_t* kout = (uint32_t*)ctx->fkey_alt.p;
+        uint32_t *vin = (uint32_t*)ctx->dperm.p, *vout = (uint32_t*)ctx->dperm_alt.p;
+        CUB([&](void* t, size_t& b) {
+            return cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int)L, 0, end_bit, ctx->st);
+        });
+        ctx->launches += (uint64_t)launch_transpose_fill(ctx->st, vout, (const uint32_t*)ctx->lrows.p,
+                                                         (const float*)ctx->w.p, L, (uint2*)ctx->ft.p);
+        ctx->launches += (uint64_t)launch_csr_starts(ctx->st, kout, L, nc, (uint32_t*)ctx->ftstarts.p);
+    } else {
+        CK(cudaMemsetAsync(ctx->ftstarts.p, 0, ((size_t)nc + 1) * 4, ctx->st));
+    }
+    CKL();
+    // 6. Cluster of every surfel (all ones: in no cluster).
+    ENSURE(ctx->cid, (size_t)n * 4);
+    CK(cudaMemsetAsync(ctx->cid.p, 0xff, (size_t)n * 4, ctx->st));
+    ctx->launches += (uint64_t)launch_cluster_ids(ctx->st, (const uint2*)ctx->crange.p,
+                                                  (const uint32_t*)ctx->members.p, nc, (uint32_t*)ctx->cid.p);
+    CKL();
+    // 7. Work buffers.
+    ENSURE(ctx->hist, (size_t)n * 16 * (bounces > 1 ? bounces - 1 : 1));
+    ENSURE(ctx->cluster_rad, (size_t)nc * 16);
+    ENSURE(ctx->dg, (size_t)px * 12);
+    ENSURE(ctx->h_t, (size_t)n * 16);
+    ENSURE(ctx->yv, (size_t)nc * 16);
+    ENSURE(ctx->ebar, (size_t)n * 16);
+    ENSURE(ctx->rhobar, (size_t)n * 16);
+    const uint32_t chunks = (px + kEmitChunk - 1) / kEmitChunk + (n + kEmitChunk - 1) / kEmitChunk;
+    ENSURE(ctx->epart, (size_t)(nl ? nl : 1) * chunks * 12);
+    ENSURE(ctx->eout, (size_t)(nl ? nl : 1) * 12);
+    ENSURE(ctx->d3, (size_t)n * 12);
+    CK(cudaStreamSynchronize(ctx->st));
+    const float ms =
+        std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    ctx->diff_P = P;
+    ctx->diff_K = bounces;
+    ctx->diff_entries = E;
+    ctx->diff_links = L;
+    ctx->diff_ready = true;
+    if (out) *out = ifx_diff_info{n, nl, px, E, L, bounces, ms};
+    return IFX_OK;
+}
+
+extern "C" int ifx_diff_forward(ifx_ctx* ctx, const float* rho, const float* emit, float* image) {
+    if (!ctx || !ctx->diff_ready) return fail(ctx, IFX_ERR_INVALID, "no prepared differentiable frame");
+    CK(cudaSetDevice(ctx->device));
+    int r;
+    if (rho && (r = ifx_surfels_set_albedo(ctx, rho))) return r;
+    if (emit && (r = ifx_lights_set_emission(ctx, ctx->nl, emit))) return r;
+    const uint32_t n = ctx->n, K = ctx->diff_K;
+    SurfelArrays s = ctx->sarr();
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    ctx->launches += (uint64_t)launch_relight(ctx->st, s.albedo, (const float*)ctx->dterms.p,
+                                              (const float4*)ctx->lemit.p, (int)ctx->nl, n, s.direct, s.rad, s.irr);
+    SolveCtl* ctl = (SolveCtl*)ctx->ctl.p;
+    CK(cudaMemsetAsync(ctl, 0, sizeof(SolveCtl), ctx->st));
+    for (uint32_t it = 0; it < K; ++it) {
+        // irr_k of every bounce but the last goes to the history; the last
+        // lands in the surfels' irr, which the frame gathers.
+        SurfelArrays b = s;
+        if (it + 1 < K) b.irr = (float4*)ctx->hist.p + (size_t)it * n;
+        int l = 0;
+        launch_solve_bounce(ctx->st, b, n, (const float4*)ctx->cp.p, (const uint2*)ctx->crange.p,
+                            (const uint32_t*)ctx->members.p, ctx->nc, (const uint32_t*)ctx->starts.p,
+                            (const uint32_t*)ctx->idx.p, (const float*)ctx->w.p, (float4*)ctx->cluster_rad.p, ctl,
+                            it, &l, 1);
+        ctx->launches += (uint64_t)l;
+    }
+    ctx->launches += (uint64_t)launch_grid_refresh(ctx->st, (const uint32_t*)ctx->gitems.p, s.irr, n,
+                                                   (float4*)ctx->girr.p);
+    ctx->launches += (uint64_t)launch_compose(ctx->st, ctx->diff_P);
+    CKL();
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    const size_t px = (size_t)ctx->diff_P.w * ctx->diff_P.h;
+    if (image) CK(cudaMemcpyAsync(image, ctx->film.p, px * 12, cudaMemcpyDeviceToHost, ctx->st));
+    if ((r = check_status(ctx))) return r;
+    CK(cudaEventElapsedTime(&ctx->stats.ms_diff_forward, ctx->ev0, ctx->ev1));
+    return IFX_OK;
+}
+
+extern "C" int ifx_diff_backward(ifx_ctx* ctx, const float* grad_image, float* grad_rho, float* grad_emit) {
+    if (!ctx || !ctx->diff_ready) return fail(ctx, IFX_ERR_INVALID, "no prepared differentiable frame");
+    if (!grad_image) return fail(ctx, IFX_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    const uint32_t n = ctx->n, nc = ctx->nc, nl = ctx->nl, K = ctx->diff_K;
+    const uint32_t px = ctx->diff_P.w * ctx->diff_P.h;
+    CK(cudaMemcpyAsync(ctx->dg.p, grad_image, (size_t)px * 12, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    const float4* alb = (const float4*)ctx->salb.p;
+    float4* t = (float4*)ctx->h_t.p;
+    ctx->launches += (uint64_t)launch_gather_t(ctx->st, (const uint32_t*)ctx->gtstarts.p,
+                                               (const float4*)ctx->gent.p, (const float*)ctx->dg.p, n, t);
+    for (uint32_t k = K; k >= 1; --k) {
+        ctx->launches += (uint64_t)launch_ft_spmv(ctx->st, (const uint32_t*)ctx->ftstarts.p, (const uint2*)ctx->ft.p,
+                                                  t, nc, (float4*)ctx->yv.p);
+        const float4* prev = k >= 2 ? (const float4*)ctx->hist.p + (size_t)(k - 2) * n : nullptr;
+        ctx->launches += (uint64_t)launch_adj_surfel(ctx->st, (const uint32_t*)ctx->cid.p, (const float4*)ctx->sp.p,
+                                                     (const float4*)ctx->cp.p, (const float4*)ctx->yv.p, alb, prev, n,
+                                                     k == K ? 1 : 0, (float4*)ctx->ebar.p,
+                                                     (float4*)ctx->rhobar.p, t);
+    }
+    ctx->launches += (uint64_t)launch_adj_final(ctx->st, (const float4*)ctx->ebar.p, alb,
+                                                (const float*)ctx->dterms.p, (const float4*)ctx->lemit.p, (int)nl,
+                                                n, (float4*)ctx->rhobar.p);
+    if (nl)
+        ctx->launches += (uint64_t)launch_emit_grad(ctx->st, (const float4*)ctx->dpix.p, (const float*)ctx->dg.p,
+                                                    px, (const float4*)ctx->ebar.p, alb,
+                                                    (const float*)ctx->dterms.p, n, (int)nl, (float*)ctx->epart.p,
+                                                    (float*)ctx->eout.p);
+    ctx->launches += (uint64_t)launch_unpack3(ctx->st, (const float4*)ctx->rhobar.p, n, (float*)ctx->d3.p);
+    CKL();
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    if (grad_rho) CK(cudaMemcpyAsync(grad_rho, ctx->d3.p, (size_t)n * 12, cudaMemcpyDeviceToHost, ctx->st));
+    if (grad_emit && nl) CK(cudaMemcpyAsync(grad_emit, ctx->eout.p, (size_t)nl * 12, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaEventElapsedTime(&ctx->stats.ms_diff_backward, ctx->ev0, ctx->ev1));
     return IFX_OK;
 }

@@ -898,12 +898,17 @@ __device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DM
 }
 
 // shade.rs:133-164
+// terms (nullable): per light, the factor ff * vis this point receives, or
+// -1 where the light is skipped (the emission-free part of each term).
 template <class C>
-__device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V albedo, uint32_t& steps_out, C& cnt) {
+__device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V albedo, uint32_t& steps_out, C& cnt,
+                                            float* terms = nullptr) {
     V out{0.0f, 0.0f, 0.0f};
     uint32_t steps = 0;
     V tan, bit;
     frame(n, tan, bit);
+    if (terms)
+        for (int li = 0; li < sv.n_lights + sv.n_slights; ++li) terms[li] = -1.0f;
     for (int li = 0; li < sv.n_lights; ++li) {
         const DQuadLight& L = sv.lights[li];
         V lc{L.center[0], L.center[1], L.center[2]};
@@ -922,6 +927,7 @@ __device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V alb
         steps += s;
         if (vis <= 1e-4f) continue;
         out = out + albedo * V{L.emit[0], L.emit[1], L.emit[2]} * (ff * vis);
+        if (terms) terms[li] = ff * vis;
     }
     for (int li = 0; li < sv.n_slights; ++li) {  // extension: sphere lights
         const DSphereLight& L = sv.slights[li];
@@ -939,13 +945,17 @@ __device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V alb
         steps += s;
         if (vis <= 1e-4f) continue;
         out = out + albedo * V{L.emit[0], L.emit[1], L.emit[2]} * (ff * vis);
+        if (terms) terms[sv.n_lights + li] = ff * vis;
     }
     steps_out = steps;
     return out;
 }
 
 // shade.rs:168-181 with trace.rs:128-148 (and sphere-light entry points).
-__device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, float tmax, V& emit) {
+// `which` (nullable) receives the index of the light picked (quad lights,
+// then sphere lights).
+__device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, float tmax, V& emit,
+                                            int* which = nullptr) {
     bool found = false;
     float best = 0.0f;
     for (int li = 0; li < sv.n_lights; ++li) {
@@ -964,6 +974,7 @@ __device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, flo
             found = true;
             best = t;
             emit = V{L.emit[0], L.emit[1], L.emit[2]};
+            if (which) *which = li;
         }
     }
     for (int li = 0; li < sv.n_slights; ++li) {
@@ -979,9 +990,17 @@ __device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, flo
             found = true;
             best = t;
             emit = V{L.emit[0], L.emit[1], L.emit[2]};
+            if (which) *which = sv.n_lights + li;
         }
     }
     return found;
+}
+
+// Emission of light l (quad lights, then sphere lights).
+__device__ __forceinline__ V light_emit(const SceneView& sv, int l) {
+    if (l < sv.n_lights) return V{sv.lights[l].emit[0], sv.lights[l].emit[1], sv.lights[l].emit[2]};
+    const DSphereLight& S = sv.slights[l - sv.n_lights];
+    return V{S.emit[0], S.emit[1], S.emit[2]};
 }
 
 // ------------------------------------------------------------ halton ------

@@ -20,10 +20,10 @@
 
 namespace ifx {
 
-static constexpr uint32_t kFlagHit = 1u << 24;
-static constexpr uint32_t kFlagDone = 1u << 25;
-static constexpr uint32_t kFlagEmit = 1u << 26;
-static constexpr uint32_t kMatMask = (1u << 24) - 1u;
+static constexpr uint32_t kFlagHit = kPixHit;
+static constexpr uint32_t kFlagDone = kPixDone;
+static constexpr uint32_t kFlagEmit = kPixEmit;
+static constexpr uint32_t kMatMask = kPixMatMask;
 
 __device__ __forceinline__ V sky() { return V{0.02f, 0.03f, 0.05f}; }
 
@@ -245,9 +245,12 @@ __global__ void __launch_bounds__(128) k_setup(ShadeParams P) {
         const bool hit = (flags & kFlagHit) != 0;
         const V rd = camera_ray(P, pix);
         V e;
-        if (emitter_hit(sv, org, rd, fminf(hit ? a.w : kMaxF, P.tmax), e)) {
+        int which = 0;
+        if (emitter_hit(sv, org, rd, fminf(hit ? a.w : kMaxF, P.tmax), e, &which)) {
             write_pixel(P, t8, pix, tonemapped ? e : V{0.9f, 0.9f, 0.9f});
-            P.hn1[pix].w = __uint_as_float(flags | kFlagDone);
+            // The light's index stays with the pixel for re-composition.
+            P.hn1[pix] = make_float4(b.x, __uint_as_float((uint32_t)which), 0.0f,
+                                     __uint_as_float(flags | kFlagDone | kFlagEmit));
             continue;
         }
         if (!hit) {
@@ -389,9 +392,10 @@ __global__ void __launch_bounds__(128) k_setup2(ShadeParams P) {
         const uint32_t flags = __float_as_uint(P.hn2[pix].w);
         const bool hit = (flags & kFlagHit) != 0;
         V e;
-        if (emitter_hit(sv, p, refl, fminf(hit ? a.w : kMaxF, P.tmax), e)) {
-            P.hp2[pix] = f4(e, a.w);
-            P.hn2[pix].w = __uint_as_float(flags | kFlagEmit);
+        int which = 0;
+        if (emitter_hit(sv, p, refl, fminf(hit ? a.w : kMaxF, P.tmax), e, &which)) {
+            P.hn2[pix] = make_float4(__uint_as_float((uint32_t)which), 0.0f, 0.0f,
+                                     __uint_as_float(flags | kFlagEmit));
             continue;
         }
         if (!hit) continue;
@@ -425,7 +429,12 @@ __global__ void __launch_bounds__(128) k_compose(ShadeParams P) {
     for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < total; pix += gridDim.x * blockDim.x) {
         const float4 b = P.hn1[pix];
         const uint32_t flags = __float_as_uint(b.w);
-        if (flags & kFlagDone) continue;
+        if (flags & kFlagDone) {
+            // Sky and debug pixels are final; an emitter pixel follows its
+            // light's current emission when the frame is re-composed.
+            if (P.recompose && (flags & kFlagEmit)) write_pixel(P, t8, pix, light_emit(sv, (int)__float_as_uint(b.y)));
+            continue;
+        }
         const V rd = camera_ray(P, pix);
         const V p = mk4(P.hp1[pix]), n = mk4(b);
         const DMaterial& m = sv.mats[flags & kMatMask];
@@ -444,7 +453,7 @@ __global__ void __launch_bounds__(128) k_compose(ShadeParams P) {
                 const uint32_t f2 = __float_as_uint(b2.w);
                 V rc;
                 if (f2 & kFlagEmit) {
-                    rc = mk4(a2);
+                    rc = light_emit(sv, (int)__float_as_uint(b2.x));
                 } else if (f2 & kFlagHit) {
                     const V p2 = mk4(a2), n2 = mk4(b2);
                     const DMaterial& m2 = sv.mats[f2 & kMatMask];
@@ -516,6 +525,14 @@ int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev) {
     if (p.counts) launch_all<Counts>(st, p, ev);
     else launch_all<NoCount>(st, p, ev);
     return p.has_gi ? 7 : 4;
+}
+
+int launch_compose(cudaStream_t st, const ShadeParams& p) {
+    const size_t sm = blob_smem(p.blob, 128);
+    ShadeParams q = p;
+    q.counts = nullptr;
+    k_compose<NoCount><<<grid_for((unsigned long long)p.w * p.h, 128, 16), 128, sm, st>>>(q);
+    return 1;
 }
 
 template <class C>

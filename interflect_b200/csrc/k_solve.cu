@@ -16,16 +16,18 @@ __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned lon
 template <class C>
 __global__ void __launch_bounds__(128) k_light_surfels(BlobRef blob, SurfelArrays s, uint32_t n,
                                                         unsigned long long* evals, uint32_t* status,
-                                                        unsigned long long* counts) {
+                                                        unsigned long long* counts, float* terms) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
     C cnt;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t limit = (n + stride - 1) / stride * stride;  // keep whole warps for the reduction
+    const int nl = sv.n_lights + sv.n_slights;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < limit; i += stride) {
         unsigned long long e = 0;
         if (i < n) {
             uint32_t steps = 0;
-            V c = direct_diffuse(sv, mk4(s.p[i]), mk4(s.n[i]), mk4(s.albedo[i]), steps, cnt);
+            V c = direct_diffuse(sv, mk4(s.p[i]), mk4(s.n[i]), mk4(s.albedo[i]), steps, cnt,
+                                 terms ? terms + (size_t)i * nl : nullptr);
             s.direct[i] = f4(c, 0.0f);
             s.rad[i] = f4(c, 0.0f);
             s.irr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -106,33 +108,34 @@ __global__ void __launch_bounds__(256) k_jacobi(float4* direct, float4* albedo, 
     if ((threadIdx.x & 31) == 0 && dmax > 0.0f) atomicMax(&ctl->residual_bits, __float_as_uint(dmax));
 }
 
-// solve.rs:454-462
-__global__ void k_bounce_end(SolveCtl* ctl, uint32_t it) {
+// solve.rs:454-462; no_exit keeps every bounce running (fixed bounce count).
+__global__ void k_bounce_end(SolveCtl* ctl, uint32_t it, int no_exit) {
     if (ctl->done) return;
     float res = __uint_as_float(ctl->residual_bits);
     ctl->iterations = it + 1;
     ctl->last_residual = ctl->residual_bits;
     ctl->residual_bits = 0;
-    if (res < 1e-4f) ctl->done = 1;
+    if (res < 1e-4f && !no_exit) ctl->done = 1;
 }
 
 void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_t n, unsigned long long* evals,
-                          uint32_t* status, unsigned long long* counts) {
+                          uint32_t* status, unsigned long long* counts, float* terms) {
     const unsigned g = grid_for(n, 128, 16);
     if (counts)
-        k_light_surfels<Counts><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, counts);
+        k_light_surfels<Counts><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, counts, terms);
     else
-        k_light_surfels<NoCount><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, nullptr);
+        k_light_surfels<NoCount><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, nullptr, terms);
 }
 
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
-                         const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches) {
+                         const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches,
+                         int no_exit) {
     k_cluster_agg<<<nc < 4096u ? nc : 4096u, kAggBlock, 0, st>>>(s.rad, s.p, cp, crange, members, nc, cluster_rad,
                                                                    ctl);
     k_jacobi<<<grid_for(n, 256), 256, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, starts, idx, w, cluster_rad,
                                                ctl);
-    k_bounce_end<<<1, 1, 0, st>>>(ctl, it);
+    k_bounce_end<<<1, 1, 0, st>>>(ctl, it, no_exit);
     *launches += 3;
 }
 

@@ -97,11 +97,14 @@ struct SolveCtl {
     uint32_t residual_bits;  // max |delta| of the bounce in progress (non-negative f32 bits)
     uint32_t last_residual;  // residual of the last completed bounce
 };
+// terms (nullable): n x nl, each surfel's per-light factor ff * vis (-1 where
+// the light is skipped), for the differentiable relight.
 void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_t n, unsigned long long* evals,
-                          uint32_t* status, unsigned long long* counts = nullptr);
+                          uint32_t* status, unsigned long long* counts = nullptr, float* terms = nullptr);
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
-                         const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches);
+                         const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches,
+                         int no_exit = 0);
 
 // ---- batched relighting (solve.rs:47-108 over R right-hand sides) ----
 int launch_batch_init(cudaStream_t st, const float* E, uint32_t n, uint32_t R, float4* direct, float4* rad,
@@ -146,23 +149,76 @@ struct ShadeParams {
     uint32_t *q1, *q2, *qr, *qlen;
     unsigned long long* cursors;
     int nl;  // quad lights + sphere lights
+    // Re-composition over stored hits (differentiable forward): emitter
+    // pixels are rewritten from the current emissions as well.
+    int recompose;
 };
 // Returns the number of kernels launched. `ev` (nullable) holds
 // kShadeEvents events recorded around the kernels (see k_shade.cu);
 // p.counts (nullable) points at 5 consecutive counter slots.
 static constexpr int kShadeEvents = 14;
 int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev);
+// k_compose alone over the hits, form factors and visibilities a previous
+// launch_shade with the same parameters left in the wavefront buffers.
+int launch_compose(cudaStream_t st, const ShadeParams& p);
+
+// ---- differentiation (k_diff.cu) ----
+// Pixel flags shared with k_shade.cu (hn1.w / hn2.w): hit, done, emitter.
+static constexpr uint32_t kPixHit = 1u << 24;
+static constexpr uint32_t kPixDone = 1u << 25;
+static constexpr uint32_t kPixEmit = 1u << 26;
+static constexpr uint32_t kPixMatMask = (1u << 24) - 1u;
+
+int launch_relight(cudaStream_t st, const float4* albedo, const float* terms, const float4* emit, int nl,
+                   uint32_t n, float4* direct, float4* rad, float4* irr);
+int launch_grid_refresh(cudaStream_t st, const uint32_t* items, const float4* irr, uint32_t n, float4* girr);
+// Pass 0: per pixel, the emission coefficients dpix[l * npix + pix] and the
+// number of gather entries cnt[pix]. Pass 1: the entries, at off[pix], as
+// (surfel, coefficient xyz + pixel in w).
+int launch_diff_pixels(cudaStream_t st, const ShadeParams& p, int pass, float4* dpix, uint32_t* cnt,
+                       const uint32_t* off, const uint32_t* gitems, uint32_t* ekey, float4* eval);
+int launch_iota(cudaStream_t st, uint32_t* v, uint32_t n);
+int launch_link_rows(cudaStream_t st, const uint32_t* starts, uint32_t n, uint32_t* rows);
+// CSR row starts (nrows + 1) from sorted row keys.
+int launch_csr_starts(cudaStream_t st, const uint32_t* sorted_keys, uint32_t count, uint32_t nrows,
+                      uint32_t* starts);
+int launch_permute_entries(cudaStream_t st, const uint32_t* perm, const float4* in, uint32_t count, float4* out);
+int launch_transpose_fill(cudaStream_t st, const uint32_t* perm, const uint32_t* link_rows, const float* w,
+                          uint32_t links, uint2* out);
+int launch_cluster_ids(cudaStream_t st, const uint2* crange, const uint32_t* members, uint32_t nc, uint32_t* cid);
+// h_i = sum over the pixels that gather surfel i of coef * dL/dimage.
+int launch_gather_t(cudaStream_t st, const uint32_t* gstarts, const float4* gent, const float* gimg, uint32_t n,
+                    float4* h);
+// y_c = sum over links (i, c) of w * t_i (the transposed transfer).
+int launch_ft_spmv(cudaStream_t st, const uint32_t* ftstarts, const uint2* ft, const float4* t, uint32_t nc,
+                   float4* y);
+// Adjoint of bounce k (K..1): b = A^T y; Ebar += b; for k >= 2
+// rhobar += b * irr_{k-1} and t = rho * b.
+int launch_adj_surfel(cudaStream_t st, const uint32_t* cid, const float4* sp, const float4* cp, const float4* y,
+                      const float4* albedo, const float4* irr_prev, uint32_t n, int first, float4* ebar,
+                      float4* rhobar, float4* t);
+// rhobar += Ebar * S (S = sum_l e_l a_il); the emission gradient from the
+// pixels (partials over fixed pixel chunks) and from the surfels, reduced in
+// a fixed order into out (nl x 3).
+int launch_adj_final(cudaStream_t st, const float4* ebar, const float4* albedo, const float* terms,
+                     const float4* emit, int nl, uint32_t n, float4* rhobar);
+static constexpr uint32_t kEmitChunk = 4096;
+int launch_emit_grad(cudaStream_t st, const float4* dpix, const float* gimg, uint32_t npix, const float4* ebar,
+                     const float4* albedo, const float* terms, uint32_t n, int nl, float* partials, float* out);
+int launch_unpack3(cudaStream_t st, const float4* in, uint32_t n, float* out);
 
 // Raises the dynamic shared-memory limit of every scene-staging kernel.
 void configure_surfel_kernels(int max_dyn_smem);
 void configure_transfer_kernels(int max_dyn_smem);
 void configure_solve_kernels(int max_dyn_smem);
 void configure_shade_kernels(int max_dyn_smem);
+void configure_diff_kernels(int max_dyn_smem);
 inline void configure_kernels(int max_dyn_smem) {
     configure_surfel_kernels(max_dyn_smem);
     configure_transfer_kernels(max_dyn_smem);
     configure_solve_kernels(max_dyn_smem);
     configure_shade_kernels(max_dyn_smem);
+    configure_diff_kernels(max_dyn_smem);
 }
 
 }  // namespace ifx

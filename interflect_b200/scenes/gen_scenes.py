@@ -20,6 +20,11 @@ Scenes (sizes as the benchmark configurations name them):
                           1920x1080, 200k surfels, 16 bounces
   c2_product_strict.rad   the same objects with reference features only: hard
                           subtraction, sphere drills, two quad lights
+  c5_cornell_fill.rad     the differentiation scene: c1_cornell at 512x512
+                          with a second, fill light (a sphere light r=0.1 of
+                          emission (2.5, 3, 4) near the open front
+                          [ext: sphere_light]), so that the gradient has two
+                          light emissions
   c3_stress.rad           512 random spheres/boxes/tori (1/3 each, size
                           U[0.1,0.5], albedo U[0.2,0.9]) in [-4,4]^3 inside an
                           enclosing box of 6 slabs, 4 quad lights of emission
@@ -76,6 +81,13 @@ def c1(rotated: bool) -> str:
     s += f'box {{ center: [0.35, -0.4, -0.3], size: [0.6, 1.2, 0.6]{rot}, mat: "white" }}\n'
     s += 'sphere { center: [-0.4, -0.65, 0.3], radius: 0.35, mat: "white" }\n'
     s += quad(0.0, 0.99, 0.0, 0.25, 0.25, (17, 12, 4))
+    return s
+
+
+def c5() -> str:
+    s = c1(True).replace("render { width: 260, height: 260,", "render { width: 512, height: 512,")
+    s = s.replace("# c1_cornell: ", "# c5_cornell_fill: ").replace("# extension: rotate_y", "# extensions: rotate_y, sphere_light")
+    s += "sphere_light { center: [-0.55, 0.55, 0.75], radius: 0.1, emit: [2.5, 3, 4] }\n"
     return s
 
 
@@ -154,7 +166,7 @@ def c3() -> str:
 
 def main() -> None:
     files = {"c1_cornell.rad": c1(True), "c1_cornell_strict.rad": c1(False), "c2_product.rad": c2(False),
-             "c2_product_strict.rad": c2(True), "c3_stress.rad": c3()}
+             "c2_product_strict.rad": c2(True), "c3_stress.rad": c3(), "c5_cornell_fill.rad": c5()}
     for name, text in files.items():
         with open(os.path.join(HERE, name), "w") as fh:
             fh.write(text)

@@ -25,6 +25,8 @@ struct orc_ctx {
     int threads = 1;
     std::string err;
     SolveStats stats{0, 0.0f};
+    DiffModel* diff = nullptr;
+    ~orc_ctx() { diff_free(diff); }
 };
 
 static void put3(float* dst, const std::vector<V3>& v) {
@@ -276,12 +278,19 @@ int orc_set_transfer(orc_ctx* c, int64_t n, const uint32_t* starts, int64_t link
 
 int64_t orc_light_surfels(orc_ctx* c) { return (int64_t)light_surfels(c->scene, c->surfels, c->threads); }
 
+int orc_solve_ex(orc_ctx* c, uint32_t max_bounces, int fixed, uint32_t* iterations, float* residual);
+
 int orc_solve(orc_ctx* c, uint32_t max_bounces, uint32_t* iterations, float* residual) {
+    return orc_solve_ex(c, max_bounces, 0, iterations, residual);
+}
+
+// fixed != 0: exactly max_bounces bounces, no residual exit.
+int orc_solve_ex(orc_ctx* c, uint32_t max_bounces, int fixed, uint32_t* iterations, float* residual) {
     if (!c->has_transfer) {
         c->err = "no transfer";
         return 1;
     }
-    c->stats = solve(c->surfels, c->transfer, max_bounces, c->threads);
+    c->stats = solve(c->surfels, c->transfer, max_bounces, c->threads, fixed != 0);
     *iterations = c->stats.iterations;
     *residual = c->stats.residual;
     return 0;
@@ -358,6 +367,50 @@ int orc_encode(orc_ctx* c, float exposure, int tonemap, uint8_t* out) {
     encode(c->film, exposure, tonemap != 0, c->srgb8);
     memcpy(out, c->srgb8.data(), c->srgb8.size());
     return 0;
+}
+
+// Per-light emission, quad lights then sphere lights, nl x 3.
+int orc_set_emission(orc_ctx* c, int64_t nl, const float* e) {
+    Scene& s = c->scene;
+    if (nl != (int64_t)(s.lights.size() + s.sphere_lights.size())) return 1;
+    size_t k = 0;
+    for (QuadLight& l : s.lights) { l.emit = V3(e[3 * k], e[3 * k + 1], e[3 * k + 2]); ++k; }
+    for (SphereLight& l : s.sphere_lights) { l.emit = V3(e[3 * k], e[3 * k + 1], e[3 * k + 2]); ++k; }
+    return 0;
+}
+
+int orc_get_emission(orc_ctx* c, float* e) {
+    size_t k = 0;
+    for (const QuadLight& l : c->scene.lights) { e[3 * k] = l.emit.x; e[3 * k + 1] = l.emit.y; e[3 * k + 2] = l.emit.z; ++k; }
+    for (const SphereLight& l : c->scene.sphere_lights) {
+        e[3 * k] = l.emit.x; e[3 * k + 1] = l.emit.y; e[3 * k + 2] = l.emit.z; ++k;
+    }
+    return 0;
+}
+
+// FP64 differentiable model (diff.cpp) of the scene camera at w x h over the
+// current surfels, transfer and grid. dims: surfels, lights, pixels.
+int orc_diff_build(orc_ctx* c, uint32_t w, uint32_t h, int64_t* dims) {
+    if (!c->has_transfer || !c->has_grid) {
+        c->err = "diff model needs a transfer and a grid";
+        return 1;
+    }
+    const Scene& s = c->scene;
+    Cam cam(s.camera.pos, s.camera.look, s.camera.up, s.camera.fov, w, h);
+    diff_free(c->diff);
+    c->diff = diff_build(s, c->surfels, c->transfer, c->grid, c->gather_radius, cam, s.diag() * 4.0f, w, h,
+                         c->threads);
+    diff_dims(*c->diff, &dims[0], &dims[1], &dims[2]);
+    return 0;
+}
+
+double orc_diff_loss(orc_ctx* c, const double* rho, const double* e, int K, const double* target, double* image) {
+    return diff_loss(*c->diff, rho, e, K, target, image);
+}
+
+double orc_diff_grad(orc_ctx* c, const double* rho, const double* e, int K, const double* target, double* g_rho,
+                     double* g_e) {
+    return diff_grad(*c->diff, rho, e, K, target, g_rho, g_e);
 }
 
 void orc_counters(int enable, int reset, uint64_t* out10) {

@@ -426,6 +426,29 @@ bool emitter_hit(const Scene& sc, V3 ro, V3 rd, float tmax, float& t_best, V3& e
     return found;
 }
 
+int emitter_index(const Scene& sc, V3 ro, V3 rd, float tmax) {
+    int best = -1, li = 0;
+    float t_best = 0.0f;
+    for (const QuadLight& l : sc.lights) {
+        float t;
+        if (intersect_quad(l.verts, ro, rd, t) && t < tmax && dot(l.normal(), rd) < 0.0f &&
+            (best < 0 || t < t_best)) {
+            best = li;
+            t_best = t;
+        }
+        ++li;
+    }
+    for (const SphereLight& l : sc.sphere_lights) {
+        float t;
+        if (intersect_sphere(l.c, l.r, ro, rd, t) && t < tmax && (best < 0 || t < t_best)) {
+            best = li;
+            t_best = t;
+        }
+        ++li;
+    }
+    return best;
+}
+
 // ------------------------------------------------------------- surfel.rs --
 void Surfels::resize(size_t k) {
     p.resize(k);
@@ -719,7 +742,7 @@ uint64_t light_surfels(const Scene& sc, Surfels& s, int threads) {
 }
 
 // solve.rs:47-108
-SolveStats solve(Surfels& s, const Transfer& t, uint32_t max_bounces, int threads) {
+SolveStats solve(Surfels& s, const Transfer& t, uint32_t max_bounces, int threads, bool no_exit) {
     size_t nc = t.nc;
     if (nc == 0) return SolveStats{0, 0.0f};
     std::vector<V3> cluster_rad(nc);
@@ -744,7 +767,7 @@ SolveStats solve(Surfels& s, const Transfer& t, uint32_t max_bounces, int thread
         residual = 0.0f;
         for (float d : deltas) residual = fmaxr(residual, d);
         iterations = it + 1;
-        if (residual < 1e-4f) break;
+        if (residual < 1e-4f && !no_exit) break;
     }
     return SolveStats{iterations, residual};
 }

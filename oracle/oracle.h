@@ -166,6 +166,9 @@ V3 diffuse_albedo(const Material& m);        // shade.rs:41-43
 V3 direct(const Scene& sc, V3 p, V3 n, V3 v, const Material& m, uint32_t& steps);  // shade.rs:50-125
 V3 direct_diffuse(const Scene& sc, V3 p, V3 n, V3 albedo, uint32_t& steps);      // shade.rs:133-164
 bool emitter_hit(const Scene& sc, V3 ro, V3 rd, float tmax, float& t, V3& emit);  // shade.rs:168-181
+// The same test returning the index of the light it picks (quad lights, then
+// sphere lights), -1 when none.
+int emitter_index(const Scene& sc, V3 ro, V3 rd, float tmax);
 
 // --------------------------------------------------------------- surfel.rs --
 struct Surfels {  // surfel.rs:23-38, stored as structure of arrays
@@ -219,7 +222,10 @@ struct SolveStats {
     float residual;
 };
 uint64_t light_surfels(const Scene& sc, Surfels& s, int threads);             // solve.rs:27-39
-SolveStats solve(Surfels& s, const Transfer& t, uint32_t max_bounces, int threads);  // solve.rs:47-108
+// no_exit: run all max_bounces bounces (the residual test never stops the
+// loop), the fixed-K form the gradient is defined on.
+SolveStats solve(Surfels& s, const Transfer& t, uint32_t max_bounces, int threads,
+                 bool no_exit = false);  // solve.rs:47-108
 
 // ----------------------------------------------------------------- main.rs --
 enum Mode : int32_t { M_BEAUTY = 0, M_DIRECT = 1, M_INDIRECT = 2, M_NORMALS = 3, M_DEPTH = 4, M_STEPS = 5 };
@@ -259,5 +265,23 @@ struct WorkCounters {
 void counters_enable(bool on);
 void counters_reset();
 WorkCounters counters_read();
+
+// ------------------------------------------------------ differentiation --
+// FP64 reference of the image as a function of per-surfel albedo rho (N x 3)
+// and per-light emission e (nl x 3) with geometry and visibility held fixed,
+// and its exact gradient (diff.cpp). Built from the current surfels
+// (positions, normals, areas), transfer and grid, for the given camera.
+struct DiffModel;
+DiffModel* diff_build(const Scene& sc, const Surfels& s, const Transfer& t, const Grid& g, float radius,
+                      const Cam& cam, float tmax, uint32_t w, uint32_t h, int threads);
+void diff_free(DiffModel* m);
+void diff_dims(const DiffModel& m, int64_t* n_surfels, int64_t* n_lights, int64_t* n_pixels);
+// Image (P x 3, may be null) and L = sum (image - target)^2 (target may be
+// null: zero) after exactly K bounces.
+double diff_loss(const DiffModel& m, const double* rho, const double* e, int K, const double* target,
+                 double* image);
+// dL/drho (N x 3) and dL/de (nl x 3); returns L.
+double diff_grad(const DiffModel& m, const double* rho, const double* e, int K, const double* target,
+                 double* g_rho, double* g_e);
 
 }  // namespace orc

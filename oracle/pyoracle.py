@@ -52,6 +52,9 @@ def lib() -> C.CDLL:
             "orc_camera": (I, [P, P, P, F, U32, U32, P]),
             "orc_render": (I64, [P, I, U32, U32, P, P, U32, U32]), "orc_get_film": (I, [P, P]),
             "orc_encode": (I, [P, F, I, P]), "orc_counters": (None, [I, I, P]),
+            "orc_solve_ex": (I, [P, U32, I, P, P]), "orc_set_emission": (I, [P, I64, P]),
+            "orc_get_emission": (I, [P, P]), "orc_diff_build": (I, [P, U32, U32, P]),
+            "orc_diff_loss": (C.c_double, [P, P, P, I, P, P]), "orc_diff_grad": (C.c_double, [P, P, P, I, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -193,12 +196,54 @@ class Oracle:
     def light_surfels(self) -> int:
         return int(lib().orc_light_surfels(self.h))
 
-    def solve(self, max_bounces: int):
+    def solve(self, max_bounces: int, fixed: bool = False):
+        """fixed: exactly max_bounces bounces (no residual exit)."""
         it = np.zeros(1, np.uint32)
         res = np.zeros(1, np.float32)
-        if lib().orc_solve(self.h, max_bounces, _p(it), _p(res)) != 0:
+        if lib().orc_solve_ex(self.h, max_bounces, 1 if fixed else 0, _p(it), _p(res)) != 0:
             raise OracleError(lib().orc_error(self.h).decode())
         return int(it[0]), float(res[0])
+
+    def set_emission(self, e) -> None:
+        """Per-light emission (quad lights, then sphere lights), nl x 3."""
+        e = f32(e).reshape(-1, 3)
+        if lib().orc_set_emission(self.h, len(e), _p(e)) != 0:
+            raise OracleError("emission count does not match the scene's lights")
+
+    def emission(self):
+        i = self.info()
+        out = np.zeros((i["lights"] + i["sphere_lights"], 3), np.float32)
+        lib().orc_get_emission(self.h, _p(out))
+        return out
+
+    def diff_build(self, width: int, height: int) -> tuple[int, int, int]:
+        """FP64 differentiable model of the scene camera; (surfels, lights, pixels)."""
+        d = np.zeros(3, np.int64)
+        if lib().orc_diff_build(self.h, width, height, _p(d)) != 0:
+            raise OracleError(lib().orc_error(self.h).decode())
+        self._diff_dims = tuple(int(v) for v in d)
+        return self._diff_dims
+
+    def diff_loss(self, rho, e, K: int, target=None):
+        """(L, image P x 3) of the FP64 model; L = sum (image - target)^2."""
+        N, nl, P = self._diff_dims
+        rho = np.ascontiguousarray(rho, np.float64).reshape(N, 3)
+        e = np.ascontiguousarray(e, np.float64).reshape(nl, 3)
+        t = None if target is None else np.ascontiguousarray(target, np.float64).reshape(P, 3)
+        img = np.zeros((P, 3), np.float64)
+        L = lib().orc_diff_loss(self.h, _p(rho), _p(e), K, _p(t), _p(img))
+        return float(L), img
+
+    def diff_grad(self, rho, e, K: int, target=None):
+        """(L, dL/drho N x 3, dL/de nl x 3) of the FP64 model."""
+        N, nl, P = self._diff_dims
+        rho = np.ascontiguousarray(rho, np.float64).reshape(N, 3)
+        e = np.ascontiguousarray(e, np.float64).reshape(nl, 3)
+        t = None if target is None else np.ascontiguousarray(target, np.float64).reshape(P, 3)
+        gr = np.zeros((N, 3), np.float64)
+        ge = np.zeros((nl, 3), np.float64)
+        L = lib().orc_diff_grad(self.h, _p(rho), _p(e), K, _p(t), _p(gr), _p(ge))
+        return float(L), gr, ge
 
     def build_grid(self):
         r = np.zeros(1, np.float32)
