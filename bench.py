@@ -42,6 +42,9 @@ WORKLOADS = {
     "c4_batch": ("interflect_b200/scenes/c1_cornell.rad",
                  "256 relighting right-hand sides (1-4 surfels-as-lights, intensity U[1,50]) on the Cornell "
                  "transfer, one CSR SpMM solve, 12 bounces max"),
+    "c4_multi": ("interflect_b200/scenes/gen_scenes.py:packed_scenes",
+                 "64 stress-style scenes (8-128 primitives, 2k-50k surfels, 256^2-1024^2 films, 24 bounces max) "
+                 "solved and shaded in one persistent cooperative launch replayed from a CUDA graph"),
     "c5_diff": ("interflect_b200/scenes/c5_cornell_fill.rad",
                 "Cornell box 512x512 with a second (fill) light, 20k surfels, 12 fixed bounces; L2 loss against a "
                 "target rendered from per-surfel albedo + N(0,0.05) clamped to [0.05,0.95]; gradient w.r.t. "
@@ -381,6 +384,105 @@ def run_batch(args, world, rank, local) -> dict | None:
     }
 
 
+def run_multi(args, world, rank, local) -> dict | None:
+    """Packed multi-scene frame: scenes/s of one graph launch over all 64
+    scenes against (a) the same scenes one packed launch each and (b) the
+    plain per-scene pipeline (light + solve + grid + render) in a loop."""
+    import interflect_b200 as ifx
+    from interflect_b200.scenes.gen_scenes import packed_scenes
+    srcs = packed_scenes(64)
+    t0 = time.time()
+    members = []
+    for src in srcs:
+        sc = ifx.parse(src)
+        ctx = ifx.Context(local)
+        ctx.upload(sc)
+        n = ctx.generate(sc.cfg.surfels)
+        info = ctx.build(8)
+        members.append((ctx, sc.cfg, n, info))
+    prep_s = time.time() - t0
+    ms = ifx.MultiScene(local)
+    for ctx, cfg, _, _ in members:
+        ms.add(ctx, cfg.width, cfg.height, cfg.bounces)
+    grid, block = ms.build(autotune=True)
+    flusher = L2Flusher(local)
+    for _ in range(args.warmup):
+        ms.run()
+    barrier(world)
+    packed = []
+    for _ in range(args.steps):
+        flusher.flush()
+        packed.append(ms.run())
+    iters = [ms.download(i, linear=False, srgb=False)[2].iterations for i in range(len(members))]
+    # (a) One packed launch per scene (the unbatched form of the same work).
+    singles = []
+    for ctx, cfg, _, _ in members:
+        one = ifx.MultiScene(local)
+        one.add(ctx, cfg.width, cfg.height, cfg.bounces)
+        one.build(autotune=False)
+        singles.append(one)
+    for one in singles:
+        one.run()
+    loop_a = []
+    for _ in range(max(1, args.steps // 3)):
+        flusher.flush()
+        loop_a.append(sum(one.run() for one in singles))
+    for one in singles:
+        one.close()
+    # (b) The plain pipeline per scene.
+    loop_b = []
+    for _ in range(max(1, args.steps // 10)):
+        tot = 0.0
+        for ctx, cfg, _, _ in members:
+            ctx.timer_start()
+            ctx.light_surfels()
+            ctx.solve(cfg.bounces)
+            ctx.grid_build()
+            ctx.render_frame(cfg.width, cfg.height, linear=False, srgb=False)
+            tot += ctx.timer_stop()
+        loop_b.append(tot)
+    # End to end: one replay plus every scene's encoded frame to the host.
+    ms = ifx.MultiScene(local)
+    for ctx, cfg, _, _ in members:
+        ms.add(ctx, cfg.width, cfg.height, cfg.bounces)
+    ms.build(autotune=False)
+    d2h = sum(cfg.width * cfg.height * 3 for _, cfg, _, _ in members)
+    e2e = []
+    for _ in range(max(1, args.steps // 3)):
+        flusher.flush()
+        t = time.perf_counter()
+        ms.run()
+        for i in range(len(members)):
+            ms.download(i, linear=False, srgb=True)
+        e2e.append((time.perf_counter() - t) * 1e3)
+    S = len(members)
+    (t_max, a_max, b_max, e_max), _ = allreduce_max_sum(
+        [statistics.median(packed), statistics.median(loop_a), statistics.median(loop_b), statistics.median(e2e)],
+        [0.0], world)
+    if rank != 0:
+        return None
+    return {
+        "metric": "packed multi-scene frames per second (solve + shade of 64 scenes in one launch)",
+        "value": S * world / (t_max / 1e3), "unit": "scenes/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "scenes": S, "description": WORKLOADS[args.workload][1],
+                   "surfels_placed_total": sum(m[2] for m in members),
+                   "links_total": sum(m[3].links for m in members),
+                   "pixels_total": sum(m[1].width * m[1].height for m in members),
+                   "bounces_run": [int(min(iters)), int(max(iters))], "launch": {"grid": grid, "block": block},
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "one_launch_per_scene": {"value": S / (a_max / 1e3), "unit": "scenes/s", "speedup": a_max / t_max},
+        "plain_pipeline_loop": {"value": S / (b_max / 1e3), "unit": "scenes/s", "speedup": b_max / t_max,
+                                "note": "ifx_light_surfels + ifx_solve + ifx_grid_build + ifx_render_frame per "
+                                        "scene (re-traces every ray)"},
+        "scene_preparation_s": prep_s,
+        "e2e": {"value": S / (e_max / 1e3), "unit": "scenes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                "includes": "graph replay and every scene's sRGB frame downloaded to host"},
+        "gpu_launches": args.steps,
+    }
+
+
 def run_diff(args, world, rank, local) -> dict | None:
     """Differentiation: one gradient step (the frame for the current albedo
     and emission, the loss gradient on the host, the adjoint) against one
@@ -557,6 +659,8 @@ def main():
             line = run_batch(args, world, rank, local)
         elif args.workload == "c5_diff":
             line = run_diff(args, world, rank, local)
+        elif args.workload == "c4_multi":
+            line = run_multi(args, world, rank, local)
         else:
             line = run_ours(args, world, rank, local)
         if line is not None:

@@ -162,6 +162,11 @@ int ifx_get_work(ifx_ctx* ctx, int kernel, uint64_t* counts, double* flops);
 /* CUDA events on the context's stream around caller-chosen work. */
 int ifx_timer_start(ifx_ctx* ctx);
 int ifx_timer_stop(ifx_ctx* ctx, float* ms);
+/* Tuning: the largest geometry program (header, objects, primitives, BVH
+ * nodes) the ray-marching kernels copy into shared memory per CTA; larger
+ * scenes are read from global memory through L1. Never changes results.
+ * Default 24 KiB, at most 160 KiB. No counterpart in the reference. */
+int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes);
 
 /* Flattens the scene (SDF object program, BVH nodes, planes, lights,
  * materials) into device memory. Must precede every stage below. */
@@ -334,6 +339,45 @@ int ifx_diff_forward(ifx_ctx* ctx, const float* rho, const float* emit, float* i
  * truncated to the same K bounces, in a fixed summation order (bit-identical
  * across runs). */
 int ifx_diff_backward(ifx_ctx* ctx, const float* grad_image, float* grad_rho, float* grad_emit);
+
+/* ------------------------------------------------- packed multi-scene --- */
+/* Many independent scenes solved and shaded in ONE persistent cooperative
+ * kernel launch, replayed from a captured CUDA graph. No counterpart in the
+ * reference (one scene per process). Each scene keeps its own context; the
+ * packed frame re-lights its surfels from the stored light factors (the
+ * result of solve::light_surfels for the context's current albedo and
+ * emission), runs solve::solve with the scene's own stop rule and bounce
+ * cap, refreshes the gather grid and re-composes every pixel from the hits,
+ * form factors and visibilities of the prepared frame. Every scene is
+ * bit-identical to ifx_light_surfels + ifx_solve + ifx_grid_build +
+ * ifx_render_frame on its own context, whatever the packing or launch shape.
+ * A context must stay alive and unused for other rendering while it belongs
+ * to a packed frame: rebuilding its transfer or grid, rendering with it or
+ * destroying it makes ifx_multiscene_run fail with IFX_ERR_INVALID.
+ * ifx_surfels_set_albedo and ifx_lights_set_emission on a member context
+ * are picked up by the next run. */
+typedef struct ifx_multiscene ifx_multiscene;
+
+int ifx_multiscene_create(int device, ifx_multiscene** out);
+void ifx_multiscene_destroy(ifx_multiscene* ms);
+const char* ifx_multiscene_last_error(const ifx_multiscene* ms);
+/* Adds ctx (scene, surfels and transfer in place, same device) with its
+ * frame: camera (NULL: the scene's), w x h, beauty mode, the scene's
+ * exposure, at most max_bounces bounces. Traces the frame once on ctx.
+ * `index` receives the scene's position. */
+int ifx_multiscene_add(ifx_multiscene* ms, ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, uint32_t h,
+                       uint32_t max_bounces, int* index);
+/* Packs the scenes, picks the launch shape (autotune != 0: times block
+ * sizes and CTAs per SM on the packed scenes and keeps the fastest; the
+ * choice never changes a bit) and captures the CUDA graph. grid and block
+ * (nullable) receive the chosen shape. */
+int ifx_multiscene_build(ifx_multiscene* ms, int autotune, int* grid, int* block);
+/* One graph launch: every scene's frame. ms_out (nullable): CUDA-event time. */
+int ifx_multiscene_run(ifx_multiscene* ms, float* ms_out);
+/* Scene `index` of the last run: linear film (w*h*3 f32), encoded frame
+ * (w*h*3 u8) and solve statistics; each nullable. */
+int ifx_multiscene_download(ifx_multiscene* ms, int index, float* out_linear, uint8_t* out_srgb,
+                            ifx_solve_stats* stats);
 
 #ifdef __cplusplus
 }

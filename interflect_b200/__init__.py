@@ -46,6 +46,8 @@ EXPORTS = (
     "ifx_solve_noalloc", "ifx_surfels_set_emission", "ifx_solve_batched", "ifx_autotune_batched",
     "ifx_surfels_set_albedo", "ifx_lights_set_emission", "ifx_lights_get_emission", "ifx_diff_setup",
     "ifx_diff_forward", "ifx_diff_backward",
+    "ifx_multiscene_create", "ifx_multiscene_destroy", "ifx_multiscene_last_error", "ifx_multiscene_add",
+    "ifx_multiscene_build", "ifx_multiscene_run", "ifx_multiscene_download", "ifx_set_stage_limit",
 )
 NOALLOC_MAX_CLUSTERS = 16384
 KERNELS = {"visibility": 0, "closure": 1, "light": 2, "primary": 3, "shadow": 4, "reflect": 5, "shadow2": 6,
@@ -157,6 +159,14 @@ def lib() -> C.CDLL:
         "ifx_diff_setup": (I, [P, C.POINTER(_Camera), U32, U32, U32, C.POINTER(_DiffInfo)]),
         "ifx_diff_forward": (I, [P, P, P, P]),
         "ifx_diff_backward": (I, [P, P, P, P]),
+        "ifx_multiscene_create": (I, [I, C.POINTER(P)]),
+        "ifx_multiscene_destroy": (None, [P]),
+        "ifx_multiscene_last_error": (C.c_char_p, [P]),
+        "ifx_multiscene_add": (I, [P, P, C.POINTER(_Camera), U32, U32, U32, C.POINTER(I)]),
+        "ifx_multiscene_build": (I, [P, I, C.POINTER(I), C.POINTER(I)]),
+        "ifx_multiscene_run": (I, [P, C.POINTER(F)]),
+        "ifx_multiscene_download": (I, [P, I, P, P, C.POINTER(_SolveStats)]),
+        "ifx_set_stage_limit": (I, [P, U32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -525,6 +535,10 @@ class Context:
         self._check(lib().ifx_get_work(self._h, KERNELS[kernel], _ptr(counts), C.byref(fl)), "get_work")
         return counts, fl.value
 
+    def set_stage_limit(self, max_bytes: int) -> None:
+        """Largest geometry program staged in shared memory per CTA (tuning only)."""
+        self._check(lib().ifx_set_stage_limit(self._h, max_bytes), "set_stage_limit")
+
     def timer_start(self) -> None:
         self._check(lib().ifx_timer_start(self._h), "timer_start")
 
@@ -552,6 +566,63 @@ def solve_noalloc(device: int, stream: int, n: int, nc: int, p_area4: int, direc
     if r != IFX_OK:
         raise DeviceError(f"ifx_solve_noalloc failed ({r}): {err.value.decode()}")
     return SolveStats(st.iterations, st.residual)
+
+
+class MultiScene:
+    """Many scenes' solve + shade in one persistent launch replayed from a
+    CUDA graph (ifx_multiscene_* in interflect.h). Member contexts must stay
+    alive, and unused for other rendering, while they belong to it."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        r = lib().ifx_multiscene_create(device, C.byref(h))
+        if r != IFX_OK:
+            raise DeviceError(f"ifx_multiscene_create(device={device}) failed with status {r}")
+        self._h = h
+        self._members: list[tuple[Context, int, int]] = []
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ifx_multiscene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, r: int, what: str) -> None:
+        if r != IFX_OK:
+            msg = lib().ifx_multiscene_last_error(self._h).decode(errors="replace")
+            if r == IFX_ERR_LIMIT:
+                raise LimitError(f"{what}: {msg}")
+            raise DeviceError(f"{what} failed ({r}): {msg}")
+
+    def add(self, ctx: Context, width: int, height: int, max_bounces: int, cam=None) -> int:
+        i = C.c_int()
+        self._check(lib().ifx_multiscene_add(self._h, ctx._h, C.byref(cam) if cam is not None else None, width,
+                                             height, max_bounces, C.byref(i)), "multiscene add")
+        self._members.append((ctx, width, height))
+        return i.value
+
+    def build(self, autotune: bool = True) -> tuple[int, int]:
+        g, b = C.c_int(), C.c_int()
+        self._check(lib().ifx_multiscene_build(self._h, 1 if autotune else 0, C.byref(g), C.byref(b)),
+                    "multiscene build")
+        return g.value, b.value
+
+    def run(self) -> float:
+        ms = C.c_float()
+        self._check(lib().ifx_multiscene_run(self._h, C.byref(ms)), "multiscene run")
+        return ms.value
+
+    def download(self, index: int, linear: bool = True, srgb: bool = True):
+        """(linear H x W x 3 | None, u8 H x W x 3 | None, SolveStats) of scene `index`."""
+        _, w, h = self._members[index]
+        lin = np.zeros((h, w, 3), np.float32) if linear else None
+        s8 = np.zeros((h, w, 3), np.uint8) if srgb else None
+        st = _SolveStats()
+        self._check(lib().ifx_multiscene_download(self._h, index, _ptr(lin), _ptr(s8), C.byref(st)),
+                    "multiscene download")
+        return lin, s8, SolveStats(st.iterations, st.residual)
 
 
 def cuda_available() -> bool:

@@ -25,10 +25,10 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "lib", "libinterflect_b200.so")
 CLI = os.path.join(HERE, "bin", "interflect")
 
-CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "k_batch.cu", "k_diff.cu", "capi.cu",
-              "noalloc.cu"]
+CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "k_batch.cu", "k_diff.cu", "k_multi.cu",
+              "capi.cu", "noalloc.cu"]
 CPP_SOURCES = ["scene_host.cpp"]
-HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh", "flop_model.h"]
+HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh", "shade.cuh", "flop_model.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",

@@ -1,6 +1,7 @@
 // C ABI (include/interflect.h): context, device memory and stage sequencing.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -28,9 +29,14 @@ struct DBuf {
     size_t cap = 0;
 };
 
-// Largest program blob staged into shared memory; bigger scenes are read
-// from global memory through the read-only cache.
-const uint32_t kMaxStagedBlob = 96 * 1024;
+// Default largest geometry program (header, objects, primitives, BVH nodes)
+// staged into shared memory per CTA; bigger scenes are read from global
+// memory through L1, which keeps more CTAs resident.
+const uint32_t kDefaultStageLimit = 24 * 1024;
+// Dynamic shared memory the scene-staging kernels may request (opt-in max).
+const int kMaxDynSmem = 227 * 1024;
+// Geometry staged plus the largest traversal stacks must fit in that.
+const uint32_t kMaxStageLimit = 160 * 1024;
 
 }  // namespace
 
@@ -47,6 +53,7 @@ struct ifx_ctx {
     HScene scene;
     DBuf blob;
     BlobRef blobref{};
+    uint32_t stage_limit = kDefaultStageLimit;
     SceneConsts sc{};
     DBuf status;  // uint32 device status word
     DBuf srgb_t;  // 256 f32 thresholds
@@ -90,6 +97,11 @@ struct ifx_ctx {
     DBuf lemit;
     uint32_t nl = 0;
 
+    // Bumped whenever the transfer, grid or wavefront buffers change: a
+    // prepared frame (differentiation, packed multi-scene) is then stale.
+    uint64_t frame_gen = 0;
+    std::vector<ifx_multiscene*> owners;  // packed frames holding this context
+
     // differentiation: the prepared frame and the transposed operators
     bool diff_ready = false;
     uint32_t diff_K = 0;
@@ -127,6 +139,11 @@ struct ifx_ctx {
 };
 
 // ------------------------------------------------------------ helpers ----
+static void frame_changed(ifx_ctx* ctx) {
+    ctx->diff_ready = false;
+    ++ctx->frame_gen;
+}
+
 static int fail(ifx_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
@@ -340,14 +357,23 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
     srgb_thresholds(t);
     if ((e = cudaMemcpyAsync(ctx->srgb_t.p, t, sizeof t, cudaMemcpyHostToDevice, ctx->st)) != cudaSuccess)
         return bail(e);
-    configure_kernels((int)kMaxStagedBlob);
+    {
+        // The opt-in maximum less room for the kernels' static shared memory.
+        int optin = kMaxDynSmem;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+        configure_kernels(std::min(optin, kMaxDynSmem) - 4096);
+        if ((e = cudaGetLastError()) != cudaSuccess) return bail(e);
+    }
     if ((e = cudaStreamSynchronize(ctx->st)) != cudaSuccess) return bail(e);
     *out = ctx;
     return IFX_OK;
 }
 
+static void multiscene_forget(ifx_multiscene* ms, ifx_ctx* ctx);
+
 extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     if (!ctx) return;
+    for (ifx_multiscene* ms : ctx->owners) multiscene_forget(ms, ctx);
     cudaSetDevice(ctx->device);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     DBuf* bufs[] = {&ctx->blob, &ctx->status, &ctx->srgb_t, &ctx->sp, &ctx->sn, &ctx->salb, &ctx->sdir, &ctx->sirr,
@@ -427,6 +453,14 @@ extern "C" int ifx_timer_stop(ifx_ctx* ctx, float* ms) {
     return IFX_OK;
 }
 
+extern "C" int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes) {
+    if (!ctx) return IFX_ERR_INVALID;
+    if (max_bytes > kMaxStageLimit) return fail(ctx, IFX_ERR_LIMIT, "stage limit above 160 KiB");
+    ctx->stage_limit = max_bytes;
+    if (ctx->has_scene) ctx->blobref.staged = ctx->blobref.stage_bytes <= max_bytes ? 1 : 0;
+    return IFX_OK;
+}
+
 extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     if (!ctx || !scene) return fail(ctx, IFX_ERR_INVALID, "null argument");
     CK(cudaSetDevice(ctx->device));
@@ -455,17 +489,18 @@ extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     if (!le.empty()) CK(cudaMemcpyAsync(ctx->lemit.p, le.data(), le.size() * 16, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     ctx->nl = (uint32_t)le.size();
-    ctx->diff_ready = false;
+    frame_changed(ctx);
     ctx->scene = s;
     ctx->blobref.ptr = (const uint8_t*)ctx->blob.p;
     ctx->blobref.bytes = (uint32_t)blob.size();
-    ctx->blobref.staged = blob.size() <= kMaxStagedBlob ? 1 : 0;
+    ctx->blobref.stage_bytes = reinterpret_cast<const BlobHeader*>(blob.data())->off_lights;
+    ctx->blobref.staged = ctx->blobref.stage_bytes <= ctx->stage_limit ? 1 : 0;
     ctx->blobref.stack_depth = maxd + 2;
     ctx->sc = scene_consts(s);
     ctx->has_scene = true;
     ctx->has_transfer = false;
     ctx->has_grid = false;
-    ctx->diff_ready = false;
+    frame_changed(ctx);
     return IFX_OK;
 }
 
@@ -510,7 +545,7 @@ extern "C" int ifx_surfels_upload(ifx_ctx* ctx, uint64_t n, const float* p, cons
     ctx->n = (uint32_t)n;
     ctx->has_transfer = false;
     ctx->has_grid = false;
-    ctx->diff_ready = false;
+    frame_changed(ctx);
     return IFX_OK;
 }
 
@@ -645,7 +680,7 @@ extern "C" int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* pla
     ctx->n = n;
     ctx->has_transfer = false;
     ctx->has_grid = false;
-    ctx->diff_ready = false;
+    frame_changed(ctx);
     if (placed) *placed = n;
     return IFX_OK;
 }
@@ -826,7 +861,7 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     ctx->links = links;
     ctx->has_transfer = true;
     ctx->has_grid = false;
-    ctx->diff_ready = false;
+    frame_changed(ctx);
     if (out) {
         float mean;
         memcpy(&mean, &hs[0], 4);
@@ -916,7 +951,7 @@ extern "C" int ifx_transfer_upload(ifx_ctx* ctx, const uint32_t* starts, uint64_
     CK(cudaStreamSynchronize(ctx->st));
     ctx->links = links;
     ctx->has_transfer = true;
-    ctx->diff_ready = false;
+    frame_changed(ctx);
     return IFX_OK;
 }
 
@@ -1160,7 +1195,7 @@ extern "C" int ifx_grid_build(ifx_ctx* ctx, float radius) {
     ctx->grid = g;
     ctx->ncells = ncells;
     ctx->has_grid = true;
-    ctx->diff_ready = false;
+    frame_changed(ctx);
     return IFX_OK;
 }
 
@@ -1270,7 +1305,7 @@ static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w
 
 extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
                                 float* out_linear, uint8_t* out_srgb, uint64_t* evals) {
-    if (ctx) ctx->diff_ready = false;  // the wavefront buffers are about to be overwritten
+    if (ctx) frame_changed(ctx);  // the wavefront buffers are about to be overwritten
     return render_impl(ctx, cam, mode, w, h, exposure, out_linear, out_srgb, evals, false, nullptr);
 }
 
@@ -1330,7 +1365,7 @@ extern "C" int ifx_diff_setup(ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, u
     if (!ctx->has_transfer || ctx->nc == 0 || ctx->n == 0) return fail(ctx, IFX_ERR_INVALID, "no transfer");
     if (bounces == 0 || bounces > 256) return fail(ctx, IFX_ERR_LIMIT, "bounces out of range (1..256)");
     CK(cudaSetDevice(ctx->device));
-    ctx->diff_ready = false;
+    frame_changed(ctx);
     const uint32_t n = ctx->n, nc = ctx->nc, nl = ctx->nl;
     const auto t_start = std::chrono::steady_clock::now();
     // 1. Each surfel's light factors (with direct = rad = E as a side effect).
@@ -1521,5 +1556,359 @@ extern "C" int ifx_diff_backward(ifx_ctx* ctx, const float* grad_image, float* g
     if (grad_emit && nl) CK(cudaMemcpyAsync(grad_emit, ctx->eout.p, (size_t)nl * 12, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     CK(cudaEventElapsedTime(&ctx->stats.ms_diff_backward, ctx->ev0, ctx->ev1));
+    return IFX_OK;
+}
+
+// ------------------------------------------------- packed multi-scene ---
+struct ifx_multiscene {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::string err;
+    struct Member {
+        ifx_ctx* ctx;
+        uint64_t gen;  // the context's frame generation when it was prepared
+        MsScene s;
+    };
+    std::vector<Member> members;
+    bool valid = true;  // false once a member context was destroyed
+    DBuf scenes, bases, ctl, live, bar, status, srgb_t;
+    MsParams params{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int grid = 0, block = 0;
+};
+
+static void multiscene_forget(ifx_multiscene* ms, ifx_ctx* ctx) {
+    for (auto& m : ms->members)
+        if (m.ctx == ctx) {
+            m.ctx = nullptr;
+            ms->valid = false;
+        }
+}
+
+static int msfail(ifx_multiscene* ms, int code, const std::string& msg) {
+    if (ms) ms->err = msg;
+    return code;
+}
+
+#define MSCK(call)                                                                                \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return msfail(ms, IFX_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+    } while (0)
+
+static int ms_ensure(ifx_multiscene* ms, DBuf& b, size_t bytes) {
+    if (b.cap >= bytes && b.p) return IFX_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    if (cudaMalloc(&b.p, bytes ? bytes : 16) != cudaSuccess) {
+        cudaGetLastError();
+        return msfail(ms, IFX_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    b.cap = bytes ? bytes : 16;
+    return IFX_OK;
+}
+
+#define MSENSURE(buf, bytes)                          \
+    do {                                              \
+        int r_ = ms_ensure(ms, (buf), (size_t)(bytes)); \
+        if (r_ != IFX_OK) return r_;                  \
+    } while (0)
+
+static void ms_drop_graph(ifx_multiscene* ms) {
+    if (ms->exec) cudaGraphExecDestroy(ms->exec);
+    if (ms->graph) cudaGraphDestroy(ms->graph);
+    ms->exec = nullptr;
+    ms->graph = nullptr;
+}
+
+extern "C" int ifx_multiscene_create(int device, ifx_multiscene** out) {
+    if (!out) return IFX_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return IFX_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return IFX_ERR_INVALID;
+    ifx_multiscene* ms = new (std::nothrow) ifx_multiscene();
+    if (!ms) return IFX_ERR_NOMEM;
+    ms->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ms->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ms->e0) != cudaSuccess || cudaEventCreate(&ms->e1) != cudaSuccess) {
+        cudaGetLastError();
+        ifx_multiscene_destroy(ms);
+        return IFX_ERR_CUDA;
+    }
+    float t[256];
+    srgb_thresholds(t);
+    if (ms_ensure(ms, ms->srgb_t, sizeof t) != IFX_OK ||
+        cudaMemcpy(ms->srgb_t.p, t, sizeof t, cudaMemcpyHostToDevice) != cudaSuccess) {
+        ifx_multiscene_destroy(ms);
+        return IFX_ERR_CUDA;
+    }
+    *out = ms;
+    return IFX_OK;
+}
+
+extern "C" void ifx_multiscene_destroy(ifx_multiscene* ms) {
+    if (!ms) return;
+    cudaSetDevice(ms->device);
+    if (ms->st) cudaStreamSynchronize(ms->st);
+    for (auto& m : ms->members)
+        if (m.ctx) {
+            auto& o = m.ctx->owners;
+            o.erase(std::remove(o.begin(), o.end(), ms), o.end());
+        }
+    ms_drop_graph(ms);
+    for (DBuf* b : {&ms->scenes, &ms->bases, &ms->ctl, &ms->live, &ms->bar, &ms->status, &ms->srgb_t}) free_buf(*b);
+    if (ms->e0) cudaEventDestroy(ms->e0);
+    if (ms->e1) cudaEventDestroy(ms->e1);
+    if (ms->st) cudaStreamDestroy(ms->st);
+    delete ms;
+}
+
+extern "C" const char* ifx_multiscene_last_error(const ifx_multiscene* ms) {
+    return ms ? ms->err.c_str() : "null packed frame";
+}
+
+extern "C" int ifx_multiscene_add(ifx_multiscene* ms, ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, uint32_t h,
+                                  uint32_t max_bounces, int* index) {
+    if (!ms || !ctx) return msfail(ms, IFX_ERR_INVALID, "null argument");
+    if (ctx->device != ms->device) return msfail(ms, IFX_ERR_INVALID, "context is on another device");
+    if (!ctx->has_scene || !ctx->has_transfer || ctx->n == 0)
+        return msfail(ms, IFX_ERR_INVALID, "context needs a scene, surfels and a transfer");
+    for (auto& m : ms->members)
+        if (m.ctx == ctx) return msfail(ms, IFX_ERR_INVALID, "context already belongs to this packed frame");
+    if (max_bounces == 0) return msfail(ms, IFX_ERR_INVALID, "max_bounces must be at least 1");
+    // Prepare through the context: light factors, grid, the frame's hits.
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return msfail(ms, IFX_ERR_CUDA, "cudaSetDevice failed");
+    const uint32_t n = ctx->n, nl = ctx->nl;
+    int r = ensure(ctx, ctx->dterms, (size_t)n * (nl ? nl : 1) * 4);
+    if (!r) {
+        launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), n, (unsigned long long*)ctx->small.p,
+                             (uint32_t*)ctx->status.p, nullptr, (float*)ctx->dterms.p);
+        ctx->launches++;
+        r = check_status(ctx);
+    }
+    if (!r) r = ifx_grid_build(ctx, 0.0f);
+    ShadeParams P{};
+    if (!r)
+        r = render_impl(ctx, cam, IFX_MODE_BEAUTY, w, h, ctx->scene.cfg.exposure, nullptr, nullptr, nullptr, true,
+                        &P);
+    if (!r) r = ensure(ctx, ctx->cluster_rad, (size_t)ctx->nc * 16);
+    if (r) return msfail(ms, r, std::string("preparing the scene: ") + ctx->err);
+    if (!P.has_gi) return msfail(ms, IFX_ERR_INVALID, "no gather grid");
+    P.counts = nullptr;
+    P.recompose = 1;
+    P.evals = nullptr;
+    MsScene s{};
+    s.sp = (const float4*)ctx->sp.p;
+    s.albedo = (const float4*)ctx->salb.p;
+    s.direct = (float4*)ctx->sdir.p;
+    s.irr = (float4*)ctx->sirr.p;
+    s.rad = (float4*)ctx->srad.p;
+    s.terms = (const float*)ctx->dterms.p;
+    s.lemit = (const float4*)ctx->lemit.p;
+    s.nl = (int)nl;
+    s.n = n;
+    s.nc = ctx->nc;
+    s.cp = (const float4*)ctx->cp.p;
+    s.crange = (const uint2*)ctx->crange.p;
+    s.members = (const uint32_t*)ctx->members.p;
+    s.starts = (const uint32_t*)ctx->starts.p;
+    s.idx = (const uint32_t*)ctx->idx.p;
+    s.w = (const float*)ctx->w.p;
+    s.crad = (float4*)ctx->cluster_rad.p;
+    s.gitems = (const uint32_t*)ctx->gitems.p;
+    s.girr = (float4*)ctx->girr.p;
+    s.max_bounces = max_bounces;
+    s.P = P;
+    ms->members.push_back({ctx, ctx->frame_gen, s});
+    ctx->owners.push_back(ms);
+    ms_drop_graph(ms);
+    if (index) *index = (int)ms->members.size() - 1;
+    return IFX_OK;
+}
+
+// Captures one packed launch of the given shape into a graph.
+static int ms_capture(ifx_multiscene* ms, int grid, int block, cudaGraphExec_t* exec, cudaGraph_t* graph) {
+    MSCK(cudaMemsetAsync(ms->bar.p, 0, sizeof(MsBarrier), ms->st));
+    MSCK(cudaStreamSynchronize(ms->st));
+    MSCK(cudaStreamBeginCapture(ms->st, cudaStreamCaptureModeThreadLocal));
+    const int lr = launch_multi_frame(ms->st, ms->params, grid, block);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(ms->st, &g);
+    if (lr < 0 || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return msfail(ms, IFX_ERR_CUDA, std::string("capturing the packed launch failed: ") + cudaGetErrorString(ce));
+    }
+    cudaGraphExec_t x = nullptr;
+    if (cudaGraphInstantiate(&x, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        return msfail(ms, IFX_ERR_CUDA, "instantiating the packed graph failed");
+    }
+    *exec = x;
+    *graph = g;
+    return IFX_OK;
+}
+
+static int ms_check(ifx_multiscene* ms) {
+    if (!ms->valid) return msfail(ms, IFX_ERR_INVALID, "a member context was destroyed");
+    for (auto& m : ms->members)
+        if (!m.ctx || m.ctx->frame_gen != m.gen)
+            return msfail(ms, IFX_ERR_INVALID, "a member context was re-rendered or rebuilt since it was added");
+    return IFX_OK;
+}
+
+static int ms_launch(ifx_multiscene* ms, cudaGraphExec_t x, float* ms_out) {
+    MSCK(cudaEventRecord(ms->e0, ms->st));
+    MSCK(cudaGraphLaunch(x, ms->st));
+    MSCK(cudaEventRecord(ms->e1, ms->st));
+    uint32_t s = 0;
+    MSCK(cudaMemcpyAsync(&s, ms->status.p, 4, cudaMemcpyDeviceToHost, ms->st));
+    MSCK(cudaStreamSynchronize(ms->st));
+    if (s) {
+        MSCK(cudaMemsetAsync(ms->status.p, 0, 4, ms->st));
+        MSCK(cudaMemsetAsync(ms->bar.p, 0, sizeof(MsBarrier), ms->st));
+        MSCK(cudaStreamSynchronize(ms->st));
+        return msfail(ms, IFX_ERR_TIMEOUT, "a grid barrier of the packed launch expired");
+    }
+    if (ms_out) MSCK(cudaEventElapsedTime(ms_out, ms->e0, ms->e1));
+    return IFX_OK;
+}
+
+extern "C" int ifx_multiscene_build(ifx_multiscene* ms, int autotune, int* grid_out, int* block_out) {
+    if (!ms) return IFX_ERR_INVALID;
+    if (ms->members.empty()) return msfail(ms, IFX_ERR_INVALID, "no scenes");
+    int r = ms_check(ms);
+    if (r) return r;
+    MSCK(cudaSetDevice(ms->device));
+    for (auto& m : ms->members) MSCK(cudaStreamSynchronize(m.ctx->st));
+    ms_drop_graph(ms);
+    const int S = (int)ms->members.size();
+    std::vector<MsScene> table(S);
+    std::vector<uint32_t> bases(3 * (size_t)S);
+    uint64_t ts = 0, tc = 0, tp = 0;
+    uint32_t maxb = 0;
+    for (int i = 0; i < S; ++i) {
+        MsScene s = ms->members[i].s;
+        s.surf_base = (uint32_t)ts;
+        s.clus_base = (uint32_t)tc;
+        s.pix_base = (uint32_t)tp;
+        bases[i] = s.surf_base;
+        bases[S + i] = s.clus_base;
+        bases[2 * S + i] = s.pix_base;
+        ts += s.n;
+        tc += s.nc;
+        tp += (uint64_t)s.P.w * s.P.h;
+        maxb = std::max(maxb, s.max_bounces);
+        table[i] = s;
+    }
+    if (ts > 0xffffffffull || tp > 0xffffffffull) return msfail(ms, IFX_ERR_LIMIT, "packed frame too large");
+    MSENSURE(ms->scenes, table.size() * sizeof(MsScene));
+    MSENSURE(ms->bases, bases.size() * 4);
+    MSENSURE(ms->ctl, (size_t)S * sizeof(SolveCtl));
+    MSENSURE(ms->live, 16);
+    MSENSURE(ms->bar, sizeof(MsBarrier));
+    MSENSURE(ms->status, 16);
+    MSCK(cudaMemcpyAsync(ms->scenes.p, table.data(), table.size() * sizeof(MsScene), cudaMemcpyHostToDevice, ms->st));
+    MSCK(cudaMemcpyAsync(ms->bases.p, bases.data(), bases.size() * 4, cudaMemcpyHostToDevice, ms->st));
+    MSCK(cudaMemsetAsync(ms->status.p, 0, 16, ms->st));
+    MSCK(cudaStreamSynchronize(ms->st));
+    MsParams& p = ms->params;
+    p.scenes = (const MsScene*)ms->scenes.p;
+    p.S = S;
+    p.surf_base = (const uint32_t*)ms->bases.p;
+    p.clus_base = p.surf_base + S;
+    p.pix_base = p.surf_base + 2 * S;
+    p.total_surf = (uint32_t)ts;
+    p.total_clus = (uint32_t)tc;
+    p.total_pix = (uint32_t)tp;
+    p.max_bounces = maxb;
+    p.ctl = (SolveCtl*)ms->ctl.p;
+    p.live = (uint32_t*)ms->live.p;
+    p.bar = (MsBarrier*)ms->bar.p;
+    p.status = (uint32_t*)ms->status.p;
+    p.srgb_t = (const float*)ms->srgb_t.p;
+    // Launch shapes: block size x CTAs per SM, never above what is resident.
+    struct Shape {
+        int grid, block;
+    };
+    std::vector<Shape> shapes;
+    int sms = 148;
+    MSCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ms->device));
+    for (int block : {128, 256}) {
+        const int maxg = multi_frame_max_blocks(block);
+        if (maxg <= 0) continue;
+        for (int per_sm = 1; per_sm * sms <= maxg; per_sm *= 2) shapes.push_back(Shape{per_sm * sms, block});
+        if (!autotune) break;
+    }
+    if (shapes.empty()) return msfail(ms, IFX_ERR_CUDA, "the packed kernel cannot be made resident");
+    if (!autotune) shapes = {shapes.back()};
+    float best = 3.4e38f;
+    Shape pick = shapes.back();
+    if (shapes.size() > 1) {
+        for (const Shape& sh : shapes) {
+            cudaGraphExec_t x = nullptr;
+            cudaGraph_t g = nullptr;
+            if ((r = ms_capture(ms, sh.grid, sh.block, &x, &g))) return r;
+            float tot = 0.0f;
+            for (int rep = 0; rep < 3 && !r; ++rep) {
+                float t = 0.0f;
+                r = ms_launch(ms, x, &t);
+                if (rep) tot += t;
+            }
+            cudaGraphExecDestroy(x);
+            cudaGraphDestroy(g);
+            if (r) return r;
+            if (tot < best) {
+                best = tot;
+                pick = sh;
+            }
+        }
+    }
+    if ((r = ms_capture(ms, pick.grid, pick.block, &ms->exec, &ms->graph))) return r;
+    ms->grid = pick.grid;
+    ms->block = pick.block;
+    if (grid_out) *grid_out = pick.grid;
+    if (block_out) *block_out = pick.block;
+    return IFX_OK;
+}
+
+extern "C" int ifx_multiscene_run(ifx_multiscene* ms, float* ms_out) {
+    if (!ms) return IFX_ERR_INVALID;
+    if (!ms->exec) return msfail(ms, IFX_ERR_INVALID, "packed frame not built");
+    int r = ms_check(ms);
+    if (r) return r;
+    MSCK(cudaSetDevice(ms->device));
+    for (auto& m : ms->members) MSCK(cudaStreamSynchronize(m.ctx->st));
+    return ms_launch(ms, ms->exec, ms_out);
+}
+
+extern "C" int ifx_multiscene_download(ifx_multiscene* ms, int index, float* out_linear, uint8_t* out_srgb,
+                                       ifx_solve_stats* stats) {
+    if (!ms) return IFX_ERR_INVALID;
+    if (index < 0 || index >= (int)ms->members.size()) return msfail(ms, IFX_ERR_INVALID, "no such scene");
+    int r = ms_check(ms);
+    if (r) return r;
+    MSCK(cudaSetDevice(ms->device));
+    const MsScene& s = ms->members[index].s;
+    const size_t px = (size_t)s.P.w * s.P.h;
+    if (out_linear) MSCK(cudaMemcpyAsync(out_linear, s.P.film, px * 12, cudaMemcpyDeviceToHost, ms->st));
+    if (out_srgb) MSCK(cudaMemcpyAsync(out_srgb, s.P.out8, px * 3, cudaMemcpyDeviceToHost, ms->st));
+    SolveCtl c{};
+    if (stats && ms->ctl.p)
+        MSCK(cudaMemcpyAsync(&c, (SolveCtl*)ms->ctl.p + index, sizeof c, cudaMemcpyDeviceToHost, ms->st));
+    MSCK(cudaStreamSynchronize(ms->st));
+    if (stats) {
+        stats->iterations = c.iterations;
+        memcpy(&stats->residual, &c.last_residual, 4);
+    }
     return IFX_OK;
 }

@@ -13,23 +13,25 @@ static constexpr unsigned kFull = 0xffffffffu;
 // Dynamic shared memory of a tracing CTA: the staged blob (when it fits)
 // followed by the threads' BVH stacks.
 static inline size_t blob_smem(const BlobRef& b, int block) {
-    size_t s = b.staged ? (size_t)align16(b.bytes) : 0;
+    size_t s = b.staged ? (size_t)align16(b.stage_bytes) : 0;
     return s + (size_t)b.stack_depth * (size_t)block * 4u;
 }
 
-// Stages the blob into dynamic shared memory (one bulk copy) or, for large
-// scenes, reads it in place, and points the view at this thread's stack.
-// All threads of the CTA must call this before any of them exits. Returns
-// false if staging timed out.
+// Stages the blob's geometry prefix into dynamic shared memory (one bulk
+// copy) or, for large scenes, reads it in place, and points the view at this
+// thread's stack. All threads of the CTA must call this before any of them
+// exits. Returns false if staging timed out.
 __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsmem, uint64_t* mbar,
                                                uint32_t* status, SceneView& sv) {
-    const uint8_t* base = blob.ptr;
+    sv = make_view(blob.ptr);
     if (blob.staged) {
-        if (!stage_scene(blob.ptr, blob.bytes, dsmem, mbar, status)) return false;
-        base = dsmem;
+        if (!stage_scene(blob.ptr, blob.stage_bytes, dsmem, mbar, status)) return false;
+        const SceneView s = make_view(dsmem);
+        sv.objs = s.objs;
+        sv.prims = s.prims;
+        sv.nodes = s.nodes;
     }
-    sv = make_view(base);
-    uint32_t* stk = reinterpret_cast<uint32_t*>(dsmem + (blob.staged ? align16(blob.bytes) : 0u));
+    uint32_t* stk = reinterpret_cast<uint32_t*>(dsmem + (blob.staged ? align16(blob.stage_bytes) : 0u));
     sv.stk = stk + threadIdx.x;
     sv.stk_stride = (int)blockDim.x;
     sv.stk_depth = blob.stack_depth;

@@ -11,11 +11,14 @@ namespace ifx {
 struct GatherView;
 
 // Program blob as handed to every tracing kernel. When `staged` is set the
-// kernel copies it into dynamic shared memory (bytes of it); otherwise it
-// reads it from global memory (large scenes).
+// kernel copies its geometry prefix (header, objects, primitives, BVH nodes:
+// the first stage_bytes bytes, all the ray marches read) into dynamic shared
+// memory; lights, materials and the linear order are always read from global
+// memory. Unstaged (large) scenes are read from global memory through L1.
 struct BlobRef {
     const uint8_t* ptr;
     uint32_t bytes;
+    uint32_t stage_bytes;
     int staged;
     int stack_depth;  // BVH traversal stack entries per thread (tree depth + 2)
 };
@@ -206,6 +209,49 @@ static constexpr uint32_t kEmitChunk = 4096;
 int launch_emit_grad(cudaStream_t st, const float4* dpix, const float* gimg, uint32_t npix, const float4* ebar,
                      const float4* albedo, const float* terms, uint32_t n, int nl, float* partials, float* out);
 int launch_unpack3(cudaStream_t st, const float4* in, uint32_t n, float* out);
+
+// ---- packed multi-scene frame (k_multi.cu) ----
+// One scene's device state, as its own context prepared it.
+struct MsScene {
+    const float4* sp;       // surfel position, w = area
+    const float4* albedo;
+    float4 *direct, *irr, *rad;
+    const float* terms;     // n x nl light factors (-1: skipped)
+    const float4* lemit;    // nl emissions
+    int nl;
+    uint32_t n, nc;
+    const float4* cp;       // cluster position, w = area
+    const uint2* crange;
+    const uint32_t* members;
+    const uint32_t *starts, *idx;
+    const float* w;
+    float4* crad;
+    const uint32_t* gitems;  // grid slot -> surfel
+    float4* girr;
+    uint32_t max_bounces;
+    uint32_t surf_base, clus_base, pix_base;  // first packed item of this scene
+    ShadeParams P;           // the prepared frame (recompose set)
+};
+struct MsBarrier {
+    uint32_t count, gen;
+};
+struct MsParams {
+    const MsScene* scenes;
+    int S;
+    const uint32_t *surf_base, *clus_base, *pix_base;  // S entries each
+    uint32_t total_surf, total_clus, total_pix;
+    uint32_t max_bounces;  // largest per-scene cap
+    SolveCtl* ctl;         // S
+    uint32_t* live;        // scenes still bouncing
+    MsBarrier* bar;
+    uint32_t* status;
+    const float* srgb_t;
+};
+// Cooperative launch (every CTA resident); capturable in a CUDA graph.
+// Returns 1, or -1 if the launch was refused.
+int launch_multi_frame(cudaStream_t st, const MsParams& p, int grid, int block);
+// Largest cooperative grid for this block size on the current device.
+int multi_frame_max_blocks(int block);
 
 // Raises the dynamic shared-memory limit of every scene-staging kernel.
 void configure_surfel_kernels(int max_dyn_smem);

@@ -130,14 +130,17 @@ def c2(strict: bool) -> str:
     return s
 
 
-def c3() -> str:
-    rng = np.random.default_rng(SEED + 3)
-    s = header("c3_stress", "512 random primitives in an enclosing box")
-    s += "render { width: 3840, height: 2160, surfels: 1000000, bounces: 24, exposure: 1.0 }\n"
+def stress_scene(rng, name: str, note: str, prims: int, surfels: int, width: int, height: int,
+                 bounces: int) -> str:
+    """The stress scene's recipe: `prims` random spheres/boxes/tori (1/3
+    each, size U[0.1,0.5], albedo U[0.2,0.9]) in [-4,4]^3 inside an enclosing
+    box of 6 slabs, 4 quad lights of emission U[5,20]."""
+    s = header(name, note)
+    s += f"render {{ width: {width}, height: {height}, surfels: {surfels}, bounces: {bounces}, exposure: 1.0 }}\n"
     s += "camera { pos: [0, 0.5, 4.3], look: [0, -0.3, 0], up: [0, 1, 0], fov: 60 }\n"
     s += 'material "wall" { albedo: [0.7, 0.7, 0.68], roughness: 0.9 }\n'
     objs = []
-    for i in range(512):
+    for i in range(prims):
         kind = rng.integers(0, 3)
         size = rng.uniform(0.1, 0.5)
         c = rng.uniform(-4.0, 4.0, 3)
@@ -162,6 +165,27 @@ def c3() -> str:
         e = rng.uniform(5.0, 20.0)
         s += quad(x, w - 0.02, z, 0.6, 0.6, (e, e, e))
     return s
+
+
+def c3() -> str:
+    return stress_scene(np.random.default_rng(SEED + 3), "c3_stress", "512 random primitives in an enclosing box",
+                        512, 1000000, 3840, 2160, 24)
+
+
+def packed_scenes(count: int = 64, seed: int = SEED + 4) -> list[str]:
+    """The batching configuration's many-scene set, generated in memory:
+    `count` scenes in the stress scene's style with 8-128 primitives,
+    2k-50k surfels requested, square films of 256..1024 pixels (multiples
+    of 64) and 24 bounces."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        prims = int(rng.integers(8, 129))
+        surfels = int(rng.integers(2000, 50001))
+        side = int(rng.integers(4, 17)) * 64
+        out.append(stress_scene(rng, f"packed_{i}", f"packed scene {i} of {count} (seed {seed})", prims, surfels,
+                                side, side, 24))
+    return out
 
 
 def main() -> None:
