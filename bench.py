@@ -45,6 +45,9 @@ WORKLOADS = {
     "c4_multi": ("interflect_b200/scenes/gen_scenes.py:packed_scenes",
                  "64 stress-style scenes (8-128 primitives, 2k-50k surfels, 256^2-1024^2 films, 24 bounces max) "
                  "solved and shaded in one persistent cooperative launch replayed from a CUDA graph"),
+    "solve_hbm": ("synthetic transfer",
+                  "Jacobi solve alone on a stress-sized synthetic transfer: 1M surfels, 3072 clusters, 109 links "
+                  "per row (109M links), 24 bounces; the HBM-bound stage measured against the copy bandwidth"),
     "c5_diff": ("interflect_b200/scenes/c5_cornell_fill.rad",
                 "Cornell box 512x512 with a second (fill) light, 20k surfels, 12 fixed bounces; L2 loss against a "
                 "target rendered from per-surfel albedo + N(0,0.05) clamped to [0.05,0.95]; gradient w.r.t. "
@@ -293,6 +296,9 @@ def run_ours(args, world, rank, local) -> dict | None:
                    "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
         "frame_ms": t_max / args.steps,
         "stage_ms": {k: statistics.mean(v) for k, v in stage.items()},
+        "solve_gbs": solve_bytes(info.links, placed, info.clusters) * st.iterations
+        / (statistics.mean(stage["solve"]) / 1e3) / 1e9,
+        "links_per_s": info.links / (statistics.mean(stage["transfer"]) / 1e3),
         "kernel_ms": avg,
         "surfel_generation_s": gen_s,
         "roofline": {"kernel": dom, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -483,6 +489,84 @@ def run_multi(args, world, rank, local) -> dict | None:
     }
 
 
+def solve_bytes(links: int, n: int, nc: int) -> int:
+    """Algorithmic bytes of one bounce: link index + weight, row starts, the
+    row's direct/albedo/rad read and irr/rad written (16 B each), the
+    members' rad + area read by the cluster means, the cluster values."""
+    return 8 * links + 4 * (n + 1) + 64 * n + 24 * nc
+
+
+def run_solve_hbm(args, world, rank, local) -> dict | None:
+    """The solve on device buffers built here (ifx_solve_noalloc runs the same
+    bounce kernels as ifx_solve), sized beyond L2 so that DRAM is exercised."""
+    import torch
+    import interflect_b200 as ifx
+    dev = torch.device(f"cuda:{local}")
+    g = torch.Generator(device=dev)
+    g.manual_seed(11)
+    n, nc, per_row, bounces = 1_000_000, 3072, 109, 24
+    L = n * per_row
+    # Surfels: position + area, direct E, albedo; clusters: a partition of the
+    # surfels into nc consecutive ranges; rows with sorted cluster indices.
+    p_area = torch.rand(n, 4, device=dev, generator=g)
+    p_area[:, 3] = 0.01
+    direct = torch.rand(n, 4, device=dev, generator=g) * 0.1
+    albedo = torch.full((n, 4), 0.9, device=dev)
+    irr = torch.zeros(n, 4, device=dev)
+    rad = direct.clone()
+    bounds = torch.linspace(0, n, nc + 1, device=dev).round().to(torch.int64)
+    ranges = torch.stack([bounds[:-1], bounds[1:]], 1).to(torch.int32).contiguous()
+    members = torch.arange(n, device=dev, dtype=torch.int32)
+    cp = torch.zeros(nc, 4, device=dev)
+    cp[:, 3] = (bounds[1:] - bounds[:-1]).to(torch.float32) * 0.01
+    starts = (torch.arange(n + 1, device=dev, dtype=torch.int64) * per_row).to(torch.int32)
+    idx = torch.sort(torch.randint(0, nc, (n, per_row), device=dev, generator=g, dtype=torch.int32), dim=1)[0]
+    idx = idx.reshape(-1).contiguous()
+    w = (torch.rand(L, device=dev, generator=g) * (0.98 / per_row * 2)).contiguous()
+    stream = torch.cuda.current_stream(dev)
+
+    def once():
+        rad.copy_(direct)
+        return ifx.solve_noalloc(local, stream.cuda_stream, n, nc, p_area.data_ptr(), direct.data_ptr(),
+                                 albedo.data_ptr(), irr.data_ptr(), rad.data_ptr(), cp.data_ptr(),
+                                 ranges.data_ptr(), members.data_ptr(), starts.data_ptr(), idx.data_ptr(),
+                                 w.data_ptr(), bounces)
+
+    for _ in range(args.warmup):
+        st = once()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        st = once()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    (t_max,), _ = allreduce_max_sum([statistics.median(times)], [0.0], world)
+    if rank != 0:
+        return None
+    bpb = solve_bytes(L, n, nc)
+    gbs = bpb * st.iterations / (t_max / 1e3) / 1e9
+    peak = measured_peaks().get("hbm_gbs", 6650.0)
+    traffic = None
+    tj = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tj):
+        with open(tj) as f:
+            traffic = json.load(f).get(args.workload, {}).get("jacobi")
+    return {
+        "metric": "Jacobi solve bandwidth (algorithmic bytes per bounce x bounces / time)", "value": gbs * world,
+        "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "surfels": n, "clusters": nc, "links": L, "bounces_run": st.iterations,
+                   "bytes_per_bounce": bpb, "l2": "working set 0.94 GB per bounce, 7x the 126 MB L2"},
+        "roofline": {"kernel": "k_jacobi + k_cluster_agg", "bound": "hbm", "achieved": gbs, "peak": peak,
+                     "unit": "GB/s", "frac": gbs / peak, "traffic": traffic,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"},
+        "gpu_launches": 3 * st.iterations * args.steps,
+    }
+
+
 def run_diff(args, world, rank, local) -> dict | None:
     """Differentiation: one gradient step (the frame for the current albedo
     and emission, the loss gradient on the host, the adjoint) against one
@@ -659,6 +743,8 @@ def main():
             line = run_batch(args, world, rank, local)
         elif args.workload == "c5_diff":
             line = run_diff(args, world, rank, local)
+        elif args.workload == "solve_hbm":
+            line = run_solve_hbm(args, world, rank, local)
         elif args.workload == "c4_multi":
             line = run_multi(args, world, rank, local)
         else:

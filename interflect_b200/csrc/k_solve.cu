@@ -84,19 +84,51 @@ __global__ void __launch_bounds__(kAggBlock) k_cluster_agg(const float4* rad, co
     }
 }
 
-// solve.rs:76-102: one Jacobi row per thread, links summed in CSR order;
-// the bounce residual is the maximum change over rows, an order-free
-// reduction kept as the bits of a non-negative f32 (NaN ignored, as the
-// reference's f32::max fold does).
-__global__ void __launch_bounds__(256) k_jacobi(float4* direct, float4* albedo, float4* irr_out, float4* rad,
-                                                 uint32_t n, const uint32_t* starts, const uint32_t* idx,
-                                                 const float* w, const float4* cluster_rad, SolveCtl* ctl) {
+// solve.rs:76-102: one Jacobi row per thread, its links added in CSR order
+// (the reference's sum). Each iteration of the row loop issues the index and
+// weight loads of 8 links as two 128-bit loads each, then the 8 cluster
+// gathers, before the first add, so a thread keeps 12 loads in flight; the
+// products crad[idx] * w and their left-to-right sum round exactly as the
+// scalar loop does. `vec` is 0 when idx or w is not 16-byte aligned (caller-
+// provided arrays), which keeps every load scalar. The bounce residual is the
+// maximum change over rows, an order-free reduction kept as the bits of a
+// non-negative f32 (NaN ignored, as the reference's f32::max fold does).
+static constexpr int kJacBlock = 256;
+__device__ __forceinline__ V jacobi_row(const float4* __restrict__ crad, const uint32_t* __restrict__ idx,
+                                        const float* __restrict__ w, uint32_t k, uint32_t e, int vec) {
+    V irr{0.0f, 0.0f, 0.0f};
+    if (vec) {
+        for (; k < e && (k & 3u); ++k) irr = irr + mk4(__ldg(&crad[__ldg(&idx[k])])) * __ldg(&w[k]);
+        for (; k + 8 <= e; k += 8) {
+            const uint4 i0 = __ldg(reinterpret_cast<const uint4*>(idx + k));
+            const uint4 i1 = __ldg(reinterpret_cast<const uint4*>(idx + k + 4));
+            const float4 w0 = __ldg(reinterpret_cast<const float4*>(w + k));
+            const float4 w1 = __ldg(reinterpret_cast<const float4*>(w + k + 4));
+            const float4 c0 = __ldg(&crad[i0.x]), c1 = __ldg(&crad[i0.y]), c2 = __ldg(&crad[i0.z]),
+                         c3 = __ldg(&crad[i0.w]), c4 = __ldg(&crad[i1.x]), c5 = __ldg(&crad[i1.y]),
+                         c6 = __ldg(&crad[i1.z]), c7 = __ldg(&crad[i1.w]);
+            irr = irr + mk4(c0) * w0.x;
+            irr = irr + mk4(c1) * w0.y;
+            irr = irr + mk4(c2) * w0.z;
+            irr = irr + mk4(c3) * w0.w;
+            irr = irr + mk4(c4) * w1.x;
+            irr = irr + mk4(c5) * w1.y;
+            irr = irr + mk4(c6) * w1.z;
+            irr = irr + mk4(c7) * w1.w;
+        }
+    }
+    for (; k < e; ++k) irr = irr + mk4(__ldg(&crad[__ldg(&idx[k])])) * __ldg(&w[k]);
+    return irr;
+}
+
+__global__ void __launch_bounds__(kJacBlock) k_jacobi(float4* direct, float4* albedo, float4* irr_out, float4* rad,
+                                                       uint32_t n, const uint32_t* starts, const uint32_t* idx,
+                                                       const float* w, const float4* cluster_rad, SolveCtl* ctl,
+                                                       int vec) {
     if (ctl->done) return;
     float dmax = 0.0f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        V irr{0.0f, 0.0f, 0.0f};
-        const uint32_t e = starts[i + 1];
-        for (uint32_t k = starts[i]; k < e; ++k) irr = irr + mk4(__ldg(&cluster_rad[__ldg(&idx[k])])) * __ldg(&w[k]);
+        const V irr = jacobi_row(cluster_rad, idx, w, starts[i], starts[i + 1], vec);
         V nr = mk4(direct[i]) + mk4(albedo[i]) * irr;
         V diff = vabs(nr - mk4(rad[i]));
         float d = fmaxf(diff.x, fmaxf(diff.y, diff.z));
@@ -133,8 +165,9 @@ void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const floa
                          int no_exit) {
     k_cluster_agg<<<nc < 4096u ? nc : 4096u, kAggBlock, 0, st>>>(s.rad, s.p, cp, crange, members, nc, cluster_rad,
                                                                    ctl);
-    k_jacobi<<<grid_for(n, 256), 256, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, starts, idx, w, cluster_rad,
-                                               ctl);
+    const int vec = (((uintptr_t)idx | (uintptr_t)w) & 15u) == 0 ? 1 : 0;
+    k_jacobi<<<grid_for(n, kJacBlock), kJacBlock, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, starts, idx, w,
+                                                          cluster_rad, ctl, vec);
     k_bounce_end<<<1, 1, 0, st>>>(ctl, it, no_exit);
     *launches += 3;
 }
