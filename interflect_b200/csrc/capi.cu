@@ -117,8 +117,7 @@ struct ifx_ctx {
 
     // scratch
     DBuf cub_tmp, small;  // small: 8 x u64 counters / results
-    DBuf gen_cand;
-    std::vector<float4> gen_host;
+    DBuf gen_cand, gen_keep, gen_off, gen_head, gen_pts, gen_next, gen_state, gen_out;  // surfel generation
 
     // measurement: per-kernel events, work counters (4 kernels x 21 u64), timer
     cudaEvent_t kv0 = nullptr, kv1 = nullptr, kc0 = nullptr, kc1 = nullptr, tm0 = nullptr, tm1 = nullptr;
@@ -386,7 +385,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->row_scale, &ctx->row_sum, &ctx->row_sky, &ctx->row_evals, &ctx->starts, &ctx->idx,
                     &ctx->w, &ctx->cluster_rad, &ctx->ctl, &ctx->gkeys, &ctx->gkeys_alt, &ctx->gstarts, &ctx->gp,
                     &ctx->gn, &ctx->girr, &ctx->gitems, &ctx->film, &ctx->out8, &ctx->cub_tmp, &ctx->small,
-                    &ctx->gen_cand, &ctx->work, &ctx->bE, &ctx->bdirect, &ctx->brad, &ctx->birr, &ctx->bcrad,
+                    &ctx->gen_cand, &ctx->gen_keep, &ctx->gen_off, &ctx->gen_head, &ctx->gen_pts,
+                    &ctx->gen_next, &ctx->gen_state, &ctx->gen_out, &ctx->work, &ctx->bE, &ctx->bdirect, &ctx->brad, &ctx->birr, &ctx->bcrad,
                     &ctx->bdone, &ctx->biters, &ctx->bres, &ctx->blast, &ctx->bunpack, &ctx->lemit,
                     &ctx->dterms, &ctx->dpix, &ctx->dcnt, &ctx->doff, &ctx->dkey, &ctx->dkey_alt, &ctx->dperm,
                     &ctx->dperm_alt, &ctx->draw, &ctx->gent, &ctx->gtstarts, &ctx->lrows, &ctx->fkey_alt,
@@ -607,59 +607,83 @@ extern "C" int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* pla
         return v < 1 ? 1 : (v > 512 ? 512 : v);
     };
     const int dim[3] = {dim_of(0), dim_of(1), dim_of(2)};
-    auto cell_of = [&](float v, int a) {
-        float f = (v - lo[a]) * inv_cell;
-        int c = std::isnan(f) ? 0 : (f >= 2147483648.0f ? 2147483647 : (f <= -2147483648.0f ? -2147483647 - 1 : (int)f));
-        return c < 0 ? 0 : (c > dim[a] - 1 ? dim[a] - 1 : c);
-    };
     uint64_t seeds64 = (uint64_t)(uint32_t)target * 24ull;
     if (seeds64 > 0xffffffffull) seeds64 = 0xffffffffull;
     const uint32_t seeds = (uint32_t)(seeds64 < 6000000ull ? seeds64 : 6000000ull);
 
-    // Occupancy: cell -> list of accepted surfels (a hash map, since the
-    // reference's dense cell table reaches 512^3 entries).
-    std::unordered_map<uint64_t, std::vector<uint32_t>> occ;
-    std::vector<float4> acc;
-    acc.reserve((size_t)target);
+    // Seeds are projected and thinned on the GPU in batches of consecutive
+    // indices (k_surfels.cu); the host only reads each batch's counts.
     const uint32_t kChunk = 1u << 18;
+    const size_t ncells = (size_t)dim[0] * (size_t)dim[1] * (size_t)dim[2];
     ENSURE(ctx->gen_cand, (size_t)kChunk * sizeof(float4));
-    ctx->gen_host.resize(kChunk);
-    for (uint32_t s0 = 0; s0 < seeds && acc.size() < target; s0 += kChunk) {
-        uint32_t cnt = seeds - s0 < kChunk ? seeds - s0 : kChunk;
+    ENSURE(ctx->gen_keep, ((size_t)kChunk + 1) * 4);
+    ENSURE(ctx->gen_off, ((size_t)kChunk + 1) * 4);
+    ENSURE(ctx->gen_head, ncells * 4);
+    ENSURE(ctx->gen_pts, (size_t)seeds * sizeof(float4));
+    ENSURE(ctx->gen_next, (size_t)seeds * 4);
+    ENSURE(ctx->gen_state, (size_t)seeds * 4);
+    ENSURE(ctx->gen_out, (size_t)target * sizeof(float4));
+    CK(cudaMemsetAsync(ctx->gen_head.p, 0, ncells * 4, ctx->st));
+    GenGrid g{};
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = lo[a];
+        g.dim[a] = dim[a];
+    }
+    g.inv_cell = inv_cell;
+    g.d_min_sq = d_min_sq;
+    g.head = (uint32_t*)ctx->gen_head.p;
+    g.next = (uint32_t*)ctx->gen_next.p;
+    g.pts = (float4*)ctx->gen_pts.p;
+    g.state = (uint32_t*)ctx->gen_state.p;
+    g.cap = seeds;
+    g.err = (uint32_t*)ctx->status.p;
+    uint32_t* keep = (uint32_t*)ctx->gen_keep.p;
+    uint32_t* off = (uint32_t*)ctx->gen_off.p;
+    unsigned long long* small = (unsigned long long*)ctx->small.p;
+    uint32_t* undecided = (uint32_t*)&small[5];
+    uint32_t base = 0;    // points kept so far (all batches)
+    uint64_t placed_n = 0;
+    for (uint32_t s0 = 0; s0 < seeds && placed_n < target; s0 += kChunk) {
+        const uint32_t cnt = seeds - s0 < kChunk ? seeds - s0 : kChunk;
         launch_gen_project(ctx->st, ctx->blobref, ctx->sc, s0, cnt, eps, (float4*)ctx->gen_cand.p,
                            (uint32_t*)ctx->status.p);
         ctx->launches++;
+        ctx->launches += (uint64_t)launch_gen_filter(ctx->st, g, (const float4*)ctx->gen_cand.p, cnt, keep);
+        CK(cudaMemsetAsync(keep + cnt, 0, 4, ctx->st));
         CKL();
-        CK(cudaMemcpyAsync(ctx->gen_host.data(), ctx->gen_cand.p, cnt * sizeof(float4), cudaMemcpyDeviceToHost,
-                           ctx->st));
-        int r = check_status(ctx);
+        CUB([&](void* t, size_t& bb) { return cub::DeviceScan::ExclusiveSum(t, bb, keep, off, (int)cnt + 1, ctx->st); });
+        ctx->launches += (uint64_t)launch_gen_append(ctx->st, g, (const float4*)ctx->gen_cand.p, keep, off, cnt, base);
+        uint32_t kept = 0;
+        CK(cudaMemcpyAsync(&kept, off + cnt, 4, cudaMemcpyDeviceToHost, ctx->st));
+        int r = check_status(ctx);  // synchronises
         if (r) return r;
-        for (uint32_t j = 0; j < cnt && acc.size() < target; ++j) {
-            const float4 q = ctx->gen_host[j];
-            if (q.w == 0.0f) continue;
-            int c[3] = {cell_of(q.x, 0), cell_of(q.y, 1), cell_of(q.z, 2)};
-            bool close = false;
-            for (int z = std::max(c[2] - 1, 0); z <= std::min(c[2] + 1, dim[2] - 1) && !close; ++z)
-                for (int y = std::max(c[1] - 1, 0); y <= std::min(c[1] + 1, dim[1] - 1) && !close; ++y)
-                    for (int x = std::max(c[0] - 1, 0); x <= std::min(c[0] + 1, dim[0] - 1) && !close; ++x) {
-                        uint64_t key = (uint64_t)x + (uint64_t)dim[0] * ((uint64_t)y + (uint64_t)dim[1] * (uint64_t)z);
-                        auto it = occ.find(key);
-                        if (it == occ.end()) continue;
-                        for (uint32_t k : it->second) {
-                            float dx = acc[k].x - q.x, dy = acc[k].y - q.y, dz = acc[k].z - q.z;
-                            if (dx * dx + dy * dy + dz * dz < d_min_sq) {
-                                close = true;
-                                break;
-                            }
-                        }
-                    }
-            if (close) continue;
-            uint64_t key = (uint64_t)c[0] + (uint64_t)dim[0] * ((uint64_t)c[1] + (uint64_t)dim[1] * (uint64_t)c[2]);
-            occ[key].push_back((uint32_t)acc.size());
-            acc.push_back(q);
+        if (kept == 0) continue;
+        // Rounds until every point of the batch is decided; each round
+        // decides at least the earliest open point, so kept rounds suffice.
+        for (uint32_t round = 0;; ++round) {
+            if (round > kept) return fail(ctx, IFX_ERR_TIMEOUT, "Poisson thinning did not settle");
+            CK(cudaMemsetAsync(undecided, 0, 4, ctx->st));
+            ctx->launches += (uint64_t)launch_gen_resolve(ctx->st, g, base, kept, undecided);
+            CKL();
+            uint32_t open = 0;
+            CK(cudaMemcpyAsync(&open, undecided, 4, cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            if (open == 0) break;
         }
+        // Accepted points in seed order, up to the target (surfel.rs:184-186).
+        ctx->launches += (uint64_t)launch_gen_accept_flags(ctx->st, g, base, kept, keep);
+        CUB([&](void* t, size_t& bb) { return cub::DeviceScan::ExclusiveSum(t, bb, keep, off, (int)kept + 1, ctx->st); });
+        uint32_t acc_n = 0;
+        CK(cudaMemcpyAsync(&acc_n, off + kept, 4, cudaMemcpyDeviceToHost, ctx->st));
+        const uint32_t quota = (uint32_t)(target - placed_n);
+        ctx->launches += (uint64_t)launch_gen_emit(ctx->st, g, base, kept, off, quota,
+                                                   (float4*)ctx->gen_out.p + placed_n);
+        CKL();
+        if ((r = check_status(ctx))) return r;
+        placed_n += acc_n < quota ? acc_n : quota;
+        base += kept;
     }
-    const uint32_t n = (uint32_t)acc.size();
+    const uint32_t n = (uint32_t)placed_n;
     size_t b = (size_t)n * sizeof(float4);
     ENSURE(ctx->sp, b);
     ENSURE(ctx->sn, b);
@@ -667,10 +691,8 @@ extern "C" int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* pla
     ENSURE(ctx->sdir, b);
     ENSURE(ctx->sirr, b);
     ENSURE(ctx->srad, b);
-    ENSURE(ctx->gen_cand, b);
     if (n) {
-        CK(cudaMemcpyAsync(ctx->gen_cand.p, acc.data(), b, cudaMemcpyHostToDevice, ctx->st));
-        launch_gen_finalize(ctx->st, ctx->blobref, (const float4*)ctx->gen_cand.p, n, d_min * d_min / 0.65f,
+        launch_gen_finalize(ctx->st, ctx->blobref, (const float4*)ctx->gen_out.p, n, d_min * d_min / 0.65f,
                             ctx->sarr(), (uint32_t*)ctx->status.p);
         ctx->launches++;
         CKL();

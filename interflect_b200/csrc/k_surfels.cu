@@ -53,6 +53,144 @@ __global__ void __launch_bounds__(128) k_gen_finalize(BlobRef blob, const float4
     }
 }
 
+// ------------------------------------------------- Poisson-disc thinning --
+// surfel.rs:206-227 accepts seed i iff no earlier accepted surfel lies
+// within d_min (squared distance in f32, glam's dot order) and the target is
+// not yet reached; the occupancy grid there is only an accelerator, since
+// cells are d_min wide, so "within d_min" is exactly the test. Here seeds are
+// taken in batches of consecutive indices:
+//   filter   drop seeds that an accepted point of an earlier batch rejects;
+//   append   the rest become this batch's points, in seed order, linked into
+//            their occupancy cells;
+//   resolve  rounds: a point is accepted once every earlier point of the
+//            batch within d_min is rejected, and rejected as soon as one of
+//            them is accepted. Decisions are final and only taken on final
+//            information, so the fixed point is the sequential result and
+//            does not depend on scheduling; each round decides at least the
+//            earliest open point.
+// Lists are walked with a bound (the point capacity); an over-long walk sets
+// kStatusGenWalk.
+__device__ __forceinline__ int gen_cell(const GenGrid& g, float v, int a) {
+    return clampi(as_i32((v - g.lo[a]) * g.inv_cell), 0, g.dim[a] - 1);
+}
+
+__device__ __forceinline__ bool gen_close(float4 a, float4 b, float d2) {
+    const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    return dx * dx + dy * dy + dz * dz < d2;
+}
+
+// Visits every point linked into the 27 cells around p: f(index) returns
+// false to stop. Returns false if a walk hit the bound.
+template <class F>
+__device__ __forceinline__ bool gen_walk(const GenGrid& g, float4 p, F&& f) {
+    const int cx = gen_cell(g, p.x, 0), cy = gen_cell(g, p.y, 1), cz = gen_cell(g, p.z, 2);
+    for (int z = max(cz - 1, 0); z <= min(cz + 1, g.dim[2] - 1); ++z)
+        for (int y = max(cy - 1, 0); y <= min(cy + 1, g.dim[1] - 1); ++y)
+            for (int x = max(cx - 1, 0); x <= min(cx + 1, g.dim[0] - 1); ++x) {
+                const size_t cell = (size_t)x + (size_t)g.dim[0] * ((size_t)y + (size_t)g.dim[1] * (size_t)z);
+                uint32_t e = g.head[cell];
+                for (uint32_t guard = 0; e != 0; ++guard) {
+                    if (guard > g.cap) {
+                        atomicOr(g.err, kStatusGenWalk);
+                        return false;
+                    }
+                    const uint32_t idx = e - 1;
+                    if (!f(idx)) return true;
+                    e = g.next[idx];
+                }
+            }
+    return true;
+}
+
+__global__ void k_gen_filter(GenGrid g, const float4* cand, uint32_t cnt, uint32_t* keep) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+        const float4 q = cand[j];
+        bool close = false;
+        if (q.w != 0.0f)
+            gen_walk(g, q, [&](uint32_t idx) {
+                if (g.state[idx] == 1u && gen_close(g.pts[idx], q, g.d_min_sq)) close = true;
+                return !close;
+            });
+        keep[j] = (q.w != 0.0f && !close) ? 1u : 0u;
+    }
+}
+
+__global__ void k_gen_append(GenGrid g, const float4* cand, const uint32_t* keep, const uint32_t* off, uint32_t cnt,
+                             uint32_t base) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+        if (!keep[j]) continue;
+        const uint32_t pid = base + off[j];
+        if (pid >= g.cap) {
+            atomicOr(g.err, kStatusGenWalk);
+            continue;
+        }
+        const float4 q = cand[j];
+        g.pts[pid] = q;
+        g.state[pid] = 0u;
+        const size_t cell = (size_t)gen_cell(g, q.x, 0) +
+                            (size_t)g.dim[0] * ((size_t)gen_cell(g, q.y, 1) + (size_t)g.dim[1] * gen_cell(g, q.z, 2));
+        g.next[pid] = atomicExch(&g.head[cell], pid + 1u);
+    }
+}
+
+__global__ void k_gen_resolve(GenGrid g, uint32_t base, uint32_t count, uint32_t* undecided) {
+    volatile uint32_t* state = g.state;
+    uint32_t open = 0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t pid = base + k;
+        if (state[pid] != 0u) continue;
+        const float4 p = g.pts[pid];
+        bool rej = false, pend = false;
+        const bool ok = gen_walk(g, p, [&](uint32_t idx) {
+            if (idx < base || idx >= pid || !gen_close(g.pts[idx], p, g.d_min_sq)) return true;
+            const uint32_t s = state[idx];
+            if (s == 1u) rej = true;
+            else if (s == 0u) pend = true;
+            return !rej;
+        });
+        if (!ok) continue;
+        if (rej) state[pid] = 2u;
+        else if (!pend) state[pid] = 1u;
+        else ++open;
+    }
+    for (int o = 16; o >= 1; o >>= 1) open += __shfl_xor_sync(0xffffffffu, open, o);
+    if ((threadIdx.x & 31) == 0 && open) atomicAdd(undecided, open);
+}
+
+__global__ void k_gen_accept_flags(GenGrid g, uint32_t base, uint32_t count, uint32_t* flags) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= count; k += gridDim.x * blockDim.x)
+        flags[k] = k < count && g.state[base + k] == 1u ? 1u : 0u;
+}
+
+__global__ void k_gen_emit(GenGrid g, uint32_t base, uint32_t count, const uint32_t* rank, uint32_t quota,
+                           float4* out) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
+        if (g.state[base + k] == 1u && rank[k] < quota) out[rank[k]] = g.pts[base + k];
+}
+
+int launch_gen_filter(cudaStream_t st, const GenGrid& g, const float4* cand, uint32_t cnt, uint32_t* keep) {
+    k_gen_filter<<<grid_for(cnt, 256), 256, 0, st>>>(g, cand, cnt, keep);
+    return 1;
+}
+int launch_gen_append(cudaStream_t st, const GenGrid& g, const float4* cand, const uint32_t* keep,
+                      const uint32_t* off, uint32_t cnt, uint32_t base) {
+    k_gen_append<<<grid_for(cnt, 256), 256, 0, st>>>(g, cand, keep, off, cnt, base);
+    return 1;
+}
+int launch_gen_resolve(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, uint32_t* undecided) {
+    k_gen_resolve<<<grid_for(count, 256), 256, 0, st>>>(g, base, count, undecided);
+    return 1;
+}
+int launch_gen_accept_flags(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, uint32_t* flags) {
+    k_gen_accept_flags<<<grid_for((unsigned long long)count + 1, 256), 256, 0, st>>>(g, base, count, flags);
+    return 1;
+}
+int launch_gen_emit(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, const uint32_t* rank,
+                    uint32_t quota, float4* out) {
+    k_gen_emit<<<grid_for(count, 256), 256, 0, st>>>(g, base, count, rank, quota, out);
+    return 1;
+}
+
 void launch_gen_project(cudaStream_t st, BlobRef blob, SceneConsts sc, uint32_t seed0, uint32_t count, float eps,
                         float4* out, uint32_t* status) {
     k_gen_project<<<grid_for(count, 128), 128, blob_smem(blob, 128), st>>>(blob, sc, seed0, count, eps, out, status);

@@ -55,6 +55,36 @@ void launch_gen_project(cudaStream_t st, BlobRef blob, SceneConsts sc, uint32_t 
 void launch_gen_finalize(cudaStream_t st, BlobRef blob, const float4* pts, uint32_t n, float area, SurfelArrays s,
                          uint32_t* status);
 
+// Poisson-disc thinning of the projected seeds (surfel.rs:206-227) on the
+// GPU, in batches of consecutive seeds; see k_surfels.cu.
+struct GenGrid {
+    float lo[3];
+    float inv_cell;
+    int dim[3];
+    float d_min_sq;
+    uint32_t* head;       // per occupancy cell: 1 + last point inserted, 0 = empty
+    uint32_t* next;       // per point: 1 + previous point of its cell, 0 = end
+    float4* pts;          // points kept after the batch filter, in seed order
+    uint32_t* state;      // per point: 0 undecided, 1 accepted, 2 rejected
+    uint32_t cap;         // capacity of pts / next / state
+    uint32_t* err;        // device status word (bounded list walks)
+};
+static constexpr uint32_t kStatusGenWalk = 1u << 5;
+// keep[j] = seed j of the batch projected onto the surface and no accepted
+// point of an earlier batch lies within d_min of it.
+int launch_gen_filter(cudaStream_t st, const GenGrid& g, const float4* cand, uint32_t cnt, uint32_t* keep);
+// Appends the kept seeds at base + off[j] (undecided) and links them into
+// their cells.
+int launch_gen_append(cudaStream_t st, const GenGrid& g, const float4* cand, const uint32_t* keep,
+                      const uint32_t* off, uint32_t cnt, uint32_t base);
+// One round of deciding the batch's points [base, base + count) in seed
+// order; *undecided counts those still open.
+int launch_gen_resolve(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, uint32_t* undecided);
+int launch_gen_accept_flags(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, uint32_t* flags);
+// out[before + rank] = accepted point, for ranks below quota.
+int launch_gen_emit(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, const uint32_t* rank,
+                    uint32_t quota, float4* out);
+
 // ---- clusters (formfactor.rs:91-147) ----
 void launch_cluster_keys(cudaStream_t st, const float4* p, const float4* n, uint32_t count, SceneConsts sc,
                          int res, unsigned long long* keys);
