@@ -165,7 +165,7 @@ int ifx_timer_stop(ifx_ctx* ctx, float* ms);
 /* Tuning: the largest geometry program (header, objects, primitives, BVH
  * nodes) the ray-marching kernels copy into shared memory per CTA; larger
  * scenes are read from global memory through L1. Never changes results.
- * Default 24 KiB, at most 160 KiB. No counterpart in the reference. */
+ * Default 24 KiB, at most 128 KiB. No counterpart in the reference. */
 int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes);
 
 /* Flattens the scene (SDF object program, BVH nodes, planes, lights,

@@ -36,7 +36,7 @@ const uint32_t kDefaultStageLimit = 24 * 1024;
 // Dynamic shared memory the scene-staging kernels may request (opt-in max).
 const int kMaxDynSmem = 227 * 1024;
 // Geometry staged plus the largest traversal stacks must fit in that.
-const uint32_t kMaxStageLimit = 160 * 1024;
+const uint32_t kMaxStageLimit = 128 * 1024;
 
 }  // namespace
 
@@ -455,7 +455,7 @@ extern "C" int ifx_timer_stop(ifx_ctx* ctx, float* ms) {
 
 extern "C" int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes) {
     if (!ctx) return IFX_ERR_INVALID;
-    if (max_bytes > kMaxStageLimit) return fail(ctx, IFX_ERR_LIMIT, "stage limit above 160 KiB");
+    if (max_bytes > kMaxStageLimit) return fail(ctx, IFX_ERR_LIMIT, "stage limit above 128 KiB");
     ctx->stage_limit = max_bytes;
     if (ctx->has_scene) ctx->blobref.staged = ctx->blobref.stage_bytes <= max_bytes ? 1 : 0;
     return IFX_OK;

@@ -65,9 +65,12 @@ struct SceneView {
     const uint32_t* linear;
     int n_planes, n_objects, n_nodes, n_lights, n_slights, use_bvh;
     // This thread's BVH traversal stack in shared memory: entry i lives at
-    // stk[i * stk_stride]; stk_depth entries (the tree depth + 2, fixed by
-    // the host), so consecutive threads hit consecutive banks.
+    // stk[i * stk_stride] (node index) and stkd[i * stk_stride] (the node's
+    // box distance, computed when it was pushed); stk_depth entries (the tree
+    // depth + 2, fixed by the host), so consecutive threads hit consecutive
+    // banks.
     uint32_t* stk;
+    float* stkd;
     int stk_stride, stk_depth;
 };
 
@@ -75,6 +78,7 @@ __device__ __forceinline__ SceneView make_view(const uint8_t* base) {
     const BlobHeader* h = reinterpret_cast<const BlobHeader*>(base);
     SceneView v;
     v.stk = nullptr;
+    v.stkd = nullptr;
     v.stk_stride = 0;
     v.stk_depth = 0;
     v.objs = reinterpret_cast<const DObject*>(base + h->off_objects);
@@ -303,16 +307,25 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
     }
     if (sv.use_bvh) {
         if (sv.n_nodes == 0) return best;
+        // bvh.rs:100-150. A node's box distance is a pure function of p and
+        // the node, so the value computed when it was pushed (bvh.rs:135-136)
+        // is the one the reference recomputes when it pops it (:116); it is
+        // kept on the stack and counted as the reference's test.
         uint32_t* const stack = sv.stk;
+        float* const stackd = sv.stkd;
         const int stride = sv.stk_stride;
         int sp = 0;
         stack[0] = 0;
+        stackd[0] = aabb_dist(p, sv.nodes[0], cnt);
         sp = 1;
+        bool first = true;
         while (sp > 0) {
             --sp;
             const int ni = (int)stack[sp * stride];
             const DNode nd = sv.nodes[ni];
-            if (aabb_dist(p, nd, cnt) >= best.d) continue;
+            if (!first) cnt.add(CN_NODE);
+            first = false;
+            if (stackd[sp * stride] >= best.d) continue;
             if (nd.count > 0) {
                 for (int k = nd.link; k < nd.link + nd.count; ++k) {
                     const DObject o = sv.objs[k];
@@ -333,10 +346,14 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
                 if (sp + 2 > sv.stk_depth) break;
                 if (dl < dr) {
                     stack[sp * stride] = (uint32_t)r;
+                    stackd[sp * stride] = dr;
                     stack[(sp + 1) * stride] = (uint32_t)l;
+                    stackd[(sp + 1) * stride] = dl;
                 } else {
                     stack[sp * stride] = (uint32_t)l;
+                    stackd[sp * stride] = dl;
                     stack[(sp + 1) * stride] = (uint32_t)r;
+                    stackd[(sp + 1) * stride] = dr;
                 }
                 sp += 2;
             }
@@ -393,10 +410,13 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
     }
     if (sv.n_nodes == 0) return best;
     uint32_t* const stack = sv.stk;
+    float* const stackd = sv.stkd;
     const int stride = sv.stk_stride;
     int sp = 0;
+    bool first = true;
     if (active) {
         stack[0] = 0;
+        stackd[0] = aabb_dist(p, sv.nodes[0], cnt);
         sp = 1;
     }
     int pending = -1;
@@ -405,7 +425,10 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
             --sp;
             const int ni = (int)stack[sp * stride];
             const DNode nd = sv.nodes[ni];
-            if (aabb_dist(p, nd, cnt) >= best.d) continue;
+            // The box distance stored at push time (see dist_mat).
+            if (!first) cnt.add(CN_NODE);
+            first = false;
+            if (stackd[sp * stride] >= best.d) continue;
             if (nd.count > 0) {
                 pending = ni;
                 break;
@@ -419,10 +442,14 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
             }
             if (dl < dr) {
                 stack[sp * stride] = (uint32_t)r;
+                stackd[sp * stride] = dr;
                 stack[(sp + 1) * stride] = (uint32_t)l;
+                stackd[(sp + 1) * stride] = dl;
             } else {
                 stack[sp * stride] = (uint32_t)l;
+                stackd[sp * stride] = dl;
                 stack[(sp + 1) * stride] = (uint32_t)r;
+                stackd[(sp + 1) * stride] = dr;
             }
             sp += 2;
         }

@@ -14,7 +14,7 @@ static constexpr unsigned kFull = 0xffffffffu;
 // followed by the threads' BVH stacks.
 static inline size_t blob_smem(const BlobRef& b, int block) {
     size_t s = b.staged ? (size_t)align16(b.stage_bytes) : 0;
-    return s + (size_t)b.stack_depth * (size_t)block * 4u;
+    return s + (size_t)b.stack_depth * (size_t)block * 8u;  // node index + box distance
 }
 
 // Stages the blob's geometry prefix into dynamic shared memory (one bulk
@@ -33,6 +33,7 @@ __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsm
     }
     uint32_t* stk = reinterpret_cast<uint32_t*>(dsmem + (blob.staged ? align16(blob.stage_bytes) : 0u));
     sv.stk = stk + threadIdx.x;
+    sv.stkd = reinterpret_cast<float*>(stk + (size_t)blob.stack_depth * blockDim.x) + threadIdx.x;
     sv.stk_stride = (int)blockDim.x;
     sv.stk_depth = blob.stack_depth;
     return true;
