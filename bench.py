@@ -45,9 +45,9 @@ WORKLOADS = {
     "c4_multi": ("interflect_b200/scenes/gen_scenes.py:packed_scenes",
                  "64 stress-style scenes (8-128 primitives, 2k-50k surfels, 256^2-1024^2 films, 24 bounces max) "
                  "solved and shaded in one persistent cooperative launch replayed from a CUDA graph"),
-    "solve_hbm": ("synthetic transfer",
-                  "Jacobi solve alone on a stress-sized synthetic transfer: 1M surfels, 3072 clusters, 109 links "
-                  "per row (109M links), 24 bounces; the HBM-bound stage measured against the copy bandwidth"),
+    "solve_hbm": ("interflect_b200/scenes/c3_stress.rad",
+                  "Jacobi solve alone on a stress-sized transfer: the stress scene's 1M surfels and clusters with "
+                  "a synthetic CSR of 109 links per row (109M links), 24 bounces max; the HBM-bound stage"),
     "c5_diff": ("interflect_b200/scenes/c5_cornell_fill.rad",
                 "Cornell box 512x512 with a second (fill) light, 20k surfels, 12 fixed bounces; L2 loss against a "
                 "target rendered from per-surfel albedo + N(0,0.05) clamped to [0.05,0.95]; gradient w.r.t. "
@@ -497,53 +497,74 @@ def solve_bytes(links: int, n: int, nc: int) -> int:
 
 
 def run_solve_hbm(args, world, rank, local) -> dict | None:
-    """The solve on device buffers built here (ifx_solve_noalloc runs the same
-    bounce kernels as ifx_solve), sized beyond L2 so that DRAM is exercised."""
+    """The solve alone on a stress-sized transfer: the stress scene's 1M
+    surfels and clusters with a synthetic CSR of 109 links per row (sorted
+    cluster indices, seeded weights), installed with ifx_transfer_upload and
+    solved by ifx_solve (the sliced-ELL kernel). The same matrix is also
+    solved through ifx_solve_noalloc (the CSR kernel) for comparison, and the
+    two results must agree bit for bit."""
+    import numpy as np
     import torch
     import interflect_b200 as ifx
-    dev = torch.device(f"cuda:{local}")
-    g = torch.Generator(device=dev)
-    g.manual_seed(11)
-    n, nc, per_row, bounces = 1_000_000, 3072, 109, 24
+    with open(os.path.join(ROOT, "interflect_b200/scenes/c3_stress.rad")) as f:
+        scene = ifx.parse(f.read())
+    ctx = ifx.Context(local)
+    ctx.upload(scene)
+    n = ctx.generate(1_000_000)
+    nc = ctx.build_clusters(8)
+    per_row, bounces = 109, 24
     L = n * per_row
-    # Surfels: position + area, direct E, albedo; clusters: a partition of the
-    # surfels into nc consecutive ranges; rows with sorted cluster indices.
-    p_area = torch.rand(n, 4, device=dev, generator=g)
-    p_area[:, 3] = 0.01
-    direct = torch.rand(n, 4, device=dev, generator=g) * 0.1
-    albedo = torch.full((n, 4), 0.9, device=dev)
-    irr = torch.zeros(n, 4, device=dev)
-    rad = direct.clone()
-    bounds = torch.linspace(0, n, nc + 1, device=dev).round().to(torch.int64)
-    ranges = torch.stack([bounds[:-1], bounds[1:]], 1).to(torch.int32).contiguous()
-    members = torch.arange(n, device=dev, dtype=torch.int32)
-    cp = torch.zeros(nc, 4, device=dev)
-    cp[:, 3] = (bounds[1:] - bounds[:-1]).to(torch.float32) * 0.01
-    starts = (torch.arange(n + 1, device=dev, dtype=torch.int64) * per_row).to(torch.int32)
-    idx = torch.sort(torch.randint(0, nc, (n, per_row), device=dev, generator=g, dtype=torch.int32), dim=1)[0]
-    idx = idx.reshape(-1).contiguous()
-    w = (torch.rand(L, device=dev, generator=g) * (0.98 / per_row * 2)).contiguous()
-    stream = torch.cuda.current_stream(dev)
+    rng = np.random.default_rng(11)
+    idx = np.sort(rng.integers(0, nc, size=(n, per_row), dtype=np.uint32), axis=1).reshape(-1)
+    w = (rng.random(L, dtype=np.float32) * np.float32(0.98 / per_row * 2)).astype(np.float32)
+    starts = (np.arange(n + 1, dtype=np.uint64) * per_row).astype(np.uint32)
+    ctx.upload_transfer(starts, idx, w)
+    E = (rng.random((n, 3), dtype=np.float32) * np.float32(0.1)).astype(np.float32)
+    flusher = L2Flusher(local)
 
     def once():
-        rad.copy_(direct)
-        return ifx.solve_noalloc(local, stream.cuda_stream, n, nc, p_area.data_ptr(), direct.data_ptr(),
-                                 albedo.data_ptr(), irr.data_ptr(), rad.data_ptr(), cp.data_ptr(),
-                                 ranges.data_ptr(), members.data_ptr(), starts.data_ptr(), idx.data_ptr(),
-                                 w.data_ptr(), bounces)
+        ctx.set_emission(E)
+        flusher.flush()
+        st = ctx.solve(bounces)
+        return st, ctx.stats()["ms_solve"]
 
     for _ in range(args.warmup):
-        st = once()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    times = []
+        once()
+    times, st = [], None
     for _ in range(args.steps):
-        torch.cuda.synchronize()
+        st, ms = once()
+        times.append(ms)
+    rad_sell = ctx.surfels()["rad"]
+    # The CSR kernel on the same matrix (caller-owned device copies).
+    dev = torch.device(f"cuda:{local}")
+    s = ctx.surfels()
+    cl = ctx.clusters(nc)
+    t = lambda a, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(a)).to(dev, dt)
+    p_area = t(np.concatenate([s["p"], s["area"][:, None]], 1))
+    f4 = lambda a: t(np.concatenate([a, np.zeros((len(a), 1), np.float32)], 1))
+    direct, albedo, irr = f4(E), f4(s["albedo"]), torch.zeros(n, 4, device=dev)
+    rad = direct.clone()
+    cp = t(np.concatenate([cl["p"], cl["area"][:, None]], 1))
+    ranges = t(np.stack([cl["offsets"][:-1], cl["offsets"][1:]], 1).astype(np.int32), torch.int32)
+    members = t(cl["members"].astype(np.int32), torch.int32)
+    d_starts, d_idx, d_w = t(starts.astype(np.int32), torch.int32), t(idx.astype(np.int32), torch.int32), t(w)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    csr = []
+    for i in range(args.warmup + args.steps):
+        rad.copy_(direct)
+        flusher.flush()
         e0.record(stream)
-        st = once()
+        st2 = ifx.solve_noalloc(local, stream.cuda_stream, n, nc, p_area.data_ptr(), direct.data_ptr(),
+                                albedo.data_ptr(), irr.data_ptr(), rad.data_ptr(), cp.data_ptr(), ranges.data_ptr(),
+                                members.data_ptr(), d_starts.data_ptr(), d_idx.data_ptr(), d_w.data_ptr(), bounces)
         e1.record(stream)
         e1.synchronize()
-        times.append(e0.elapsed_time(e1))
-    (t_max,), _ = allreduce_max_sum([statistics.median(times)], [0.0], world)
+        if i >= args.warmup:
+            csr.append(e0.elapsed_time(e1))
+    same = bool(np.array_equal(rad[:, :3].cpu().numpy().view(np.uint32), rad_sell.view(np.uint32))) and \
+        st2.iterations == st.iterations
+    (t_max, csr_max), _ = allreduce_max_sum([statistics.median(times), statistics.median(csr)], [0.0], world)
     if rank != 0:
         return None
     bpb = solve_bytes(L, n, nc)
@@ -553,16 +574,18 @@ def run_solve_hbm(args, world, rank, local) -> dict | None:
     tj = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tj):
         with open(tj) as f:
-            traffic = json.load(f).get(args.workload, {}).get("jacobi")
+            traffic = json.load(f).get(args.workload, {}).get("jacobi_sell")
     return {
         "metric": "Jacobi solve bandwidth (algorithmic bytes per bounce x bounces / time)", "value": gbs * world,
         "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "surfels": n, "clusters": nc, "links": L, "bounces_run": st.iterations,
-                   "bytes_per_bounce": bpb, "l2": "working set 0.94 GB per bounce, 7x the 126 MB L2"},
-        "roofline": {"kernel": "k_jacobi + k_cluster_agg", "bound": "hbm", "achieved": gbs, "peak": peak,
+                   "bytes_per_bounce": bpb, "l2": "flushed before each solve; working set 7x the 126 MB L2"},
+        "roofline": {"kernel": "k_jacobi_sell + k_cluster_agg", "bound": "hbm", "achieved": gbs, "peak": peak,
                      "unit": "GB/s", "frac": gbs / peak, "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"},
+        "csr_kernel": {"value": bpb * st.iterations / (csr_max / 1e3) / 1e9, "unit": "GB/s",
+                       "ms": csr_max, "bit_identical_to_sliced_ell": same},
         "gpu_launches": 3 * st.iterations * args.steps,
     }
 

@@ -195,6 +195,10 @@ int ifx_surfels_download(ifx_ctx* ctx, float* p, float* nrm, float* albedo, floa
  * cone-traced visibility, hemisphere-closure calibration and the CSR matrix,
  * all on the GPU. */
 int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out);
+/* Replaces formfactor::build_clusters (src/formfactor.rs:91-147) alone:
+ * clusters of the current surfels, without a transfer (for example before
+ * ifx_transfer_upload installs one). `nc` receives the cluster count. */
+int ifx_clusters_build(ifx_ctx* ctx, int cluster_res, uint64_t* nc);
 /* CSR arrays: starts (n+1), idx (links), w (links). Nullable. */
 int ifx_transfer_download(ifx_ctx* ctx, uint32_t* starts, uint32_t* idx, float* w);
 /* Clusters: per cluster p(3) n(3) area radius; member offsets (nc+1) and the

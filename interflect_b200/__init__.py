@@ -48,6 +48,7 @@ EXPORTS = (
     "ifx_diff_forward", "ifx_diff_backward",
     "ifx_multiscene_create", "ifx_multiscene_destroy", "ifx_multiscene_last_error", "ifx_multiscene_add",
     "ifx_multiscene_build", "ifx_multiscene_run", "ifx_multiscene_download", "ifx_set_stage_limit",
+    "ifx_clusters_build",
 )
 NOALLOC_MAX_CLUSTERS = 16384
 KERNELS = {"visibility": 0, "closure": 1, "light": 2, "primary": 3, "shadow": 4, "reflect": 5, "shadow2": 6,
@@ -167,6 +168,7 @@ def lib() -> C.CDLL:
         "ifx_multiscene_run": (I, [P, C.POINTER(F)]),
         "ifx_multiscene_download": (I, [P, I, P, P, C.POINTER(_SolveStats)]),
         "ifx_set_stage_limit": (I, [P, U32]),
+        "ifx_clusters_build": (I, [P, I, C.POINTER(U64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -372,6 +374,12 @@ class Context:
         self._check(lib().ifx_transfer_build(self._h, cluster_res, C.byref(i)), "transfer build")
         self._tinfo = TransferInfo(i.clusters, i.links, i.candidates, i.evals, i.interior_rows, i.mean_row_sum)
         return self._tinfo
+
+    def build_clusters(self, cluster_res: int = 8) -> int:
+        """formfactor::build_clusters alone; returns the cluster count."""
+        nc = C.c_uint64()
+        self._check(lib().ifx_clusters_build(self._h, cluster_res, C.byref(nc)), "cluster build")
+        return nc.value
 
     def transfer(self) -> dict:
         k = self.n_surfels

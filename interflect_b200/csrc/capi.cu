@@ -78,6 +78,10 @@ struct ifx_ctx {
 
     // solve
     DBuf cluster_rad, ctl;
+    // the transfer in sliced-ELL form for the solve (built with the transfer)
+    DBuf sell_len, sell_perm, sell_keys, sell_rows, sell_sizes, sell_off, sell_idx, sell_w;
+    bool sell_ready = false;
+    SellMatrix sellm{};
 
     // batched relighting
     DBuf bE, bdirect, brad, birr, bcrad, bdone, biters, bres, blast, bunpack;
@@ -391,7 +395,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->dterms, &ctx->dpix, &ctx->dcnt, &ctx->doff, &ctx->dkey, &ctx->dkey_alt, &ctx->dperm,
                     &ctx->dperm_alt, &ctx->draw, &ctx->gent, &ctx->gtstarts, &ctx->lrows, &ctx->fkey_alt,
                     &ctx->ft, &ctx->ftstarts, &ctx->cid, &ctx->hist, &ctx->dg, &ctx->h_t, &ctx->yv, &ctx->ebar,
-                    &ctx->rhobar, &ctx->epart, &ctx->eout, &ctx->d3};
+                    &ctx->rhobar, &ctx->epart, &ctx->eout, &ctx->d3, &ctx->sell_len, &ctx->sell_perm, &ctx->sell_keys,
+                    &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -773,6 +778,68 @@ static int build_clusters(ifx_ctx* ctx, int res) {
     return IFX_OK;
 }
 
+// The transfer's sliced-ELL copy for the solve (kernels.h SellMatrix): rows
+// sorted by link count (stable, descending), 32-row slices, links
+// interleaved by 4 per lane. Left out (the solve reads the CSR arrays) when
+// its padded size could pass 2^32 entries.
+static int sell_build(ifx_ctx* ctx) {
+    ctx->sell_ready = false;
+    const uint32_t n = ctx->n;
+    if (n == 0 || ctx->links == 0) return IFX_OK;
+    const uint32_t ns = (n + 31) / 32;
+    ENSURE(ctx->sell_len, (size_t)n * 4);
+    ENSURE(ctx->sell_perm, (size_t)n * 4);
+    ENSURE(ctx->sell_keys, (size_t)n * 4);
+    ENSURE(ctx->sell_rows, (size_t)n * 4);
+    ENSURE(ctx->sell_sizes, ((size_t)ns + 1) * 4);
+    ENSURE(ctx->sell_off, ((size_t)ns + 1) * 4);
+    uint32_t* keys = (uint32_t*)ctx->sell_keys.p;
+    uint32_t* rows = (uint32_t*)ctx->sell_rows.p;
+    uint32_t* len = (uint32_t*)ctx->sell_len.p;
+    uint32_t* perm = (uint32_t*)ctx->sell_perm.p;
+    ctx->launches += (uint64_t)launch_sell_lens(ctx->st, (const uint32_t*)ctx->starts.p, n, keys, rows);
+    CKL();
+    CUB([&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairsDescending(t, b, keys, len, rows, perm, (int)n, 0, 32, ctx->st);
+    });
+    uint32_t maxlen = 0;
+    CK(cudaMemcpyAsync(&maxlen, len, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if ((uint64_t)ns * 32ull * (((uint64_t)maxlen + 3ull) & ~3ull) >= 0xffffffffull) return IFX_OK;
+    uint32_t* sizes = (uint32_t*)ctx->sell_sizes.p;
+    uint32_t* off = (uint32_t*)ctx->sell_off.p;
+    ctx->launches += (uint64_t)launch_sell_sizes(ctx->st, len, n, sizes);
+    CKL();
+    CUB([&](void* t, size_t& b) { return cub::DeviceScan::ExclusiveSum(t, b, sizes, off, (int)ns + 1, ctx->st); });
+    uint32_t total = 0;
+    CK(cudaMemcpyAsync(&total, off + ns, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ENSURE(ctx->sell_idx, (size_t)total * 4);
+    ENSURE(ctx->sell_w, (size_t)total * 4);
+    ctx->launches += (uint64_t)launch_sell_fill(ctx->st, (const uint32_t*)ctx->starts.p, (const uint32_t*)ctx->idx.p,
+                                                (const float*)ctx->w.p, n, perm, len, off,
+                                                (uint32_t*)ctx->sell_idx.p, (float*)ctx->sell_w.p);
+    CKL();
+    ctx->sellm = SellMatrix{perm, len, off, (const uint32_t*)ctx->sell_idx.p, (const float*)ctx->sell_w.p};
+    ctx->sell_ready = true;
+    return IFX_OK;
+}
+
+extern "C" int ifx_clusters_build(ifx_ctx* ctx, int cluster_res, uint64_t* nc) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (cluster_res < 1 || cluster_res > 512) return fail(ctx, IFX_ERR_LIMIT, "cluster resolution must be in 1..512");
+    if (ctx->n == 0) return fail(ctx, IFX_ERR_INVALID, "no surfels");
+    CK(cudaSetDevice(ctx->device));
+    int r = build_clusters(ctx, cluster_res);
+    if (r) return r;
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->has_transfer = false;
+    ctx->has_grid = false;
+    frame_changed(ctx);
+    if (nc) *nc = ctx->nc;
+    return IFX_OK;
+}
+
 extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out) {
     if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
     if (cluster_res < 1 || cluster_res > 512) return fail(ctx, IFX_ERR_LIMIT, "cluster resolution must be in 1..512");
@@ -869,6 +936,8 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     launch_sum_u64(ctx->st, (const unsigned long long*)ctx->row_evals.p, n, &small[2]);
     ctx->launches += 2;
     CKL();
+    ctx->links = links;
+    if ((r = sell_build(ctx))) return r;
     CK(cudaEventRecord(ctx->ev1, ctx->st));
     unsigned long long hs[3];
     CK(cudaMemcpyAsync(hs, small, 24, cudaMemcpyDeviceToHost, ctx->st));
@@ -957,7 +1026,7 @@ extern "C" int ifx_transfer_row_diag(ifx_ctx* ctx, float* row_sum, float* row_sk
 extern "C" int ifx_transfer_upload(ifx_ctx* ctx, const uint32_t* starts, uint64_t links, const uint32_t* idx,
                                    const float* w) {
     if (!ctx || !starts || (links && (!idx || !w))) return fail(ctx, IFX_ERR_INVALID, "null argument");
-    if (ctx->nc == 0) return fail(ctx, IFX_ERR_INVALID, "no clusters: build a transfer first");
+    if (ctx->nc == 0) return fail(ctx, IFX_ERR_INVALID, "no clusters: build clusters or a transfer first");
     if (starts[ctx->n] != links) return fail(ctx, IFX_ERR_INVALID, "starts[n] != links");
     for (uint64_t k = 0; k < links; ++k)
         if (idx[k] >= ctx->nc) return fail(ctx, IFX_ERR_INVALID, "cluster index out of range");
@@ -972,6 +1041,8 @@ extern "C" int ifx_transfer_upload(ifx_ctx* ctx, const uint32_t* starts, uint64_
     }
     CK(cudaStreamSynchronize(ctx->st));
     ctx->links = links;
+    int r = sell_build(ctx);
+    if (r) return r;
     ctx->has_transfer = true;
     frame_changed(ctx);
     return IFX_OK;
@@ -1023,7 +1094,7 @@ extern "C" int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* ou
             launch_solve_bounce(ctx->st, ctx->sarr(), ctx->n, (const float4*)ctx->cp.p, (const uint2*)ctx->crange.p,
                                 (const uint32_t*)ctx->members.p, ctx->nc, (const uint32_t*)ctx->starts.p,
                                 (const uint32_t*)ctx->idx.p, (const float*)ctx->w.p, (float4*)ctx->cluster_rad.p,
-                                ctl, it, &l);
+                                ctl, it, &l, 0, ctx->sell_ready ? &ctx->sellm : nullptr);
             ctx->launches += (uint64_t)l;
         }
         CKL();
@@ -1527,7 +1598,7 @@ extern "C" int ifx_diff_forward(ifx_ctx* ctx, const float* rho, const float* emi
         launch_solve_bounce(ctx->st, b, n, (const float4*)ctx->cp.p, (const uint2*)ctx->crange.p,
                             (const uint32_t*)ctx->members.p, ctx->nc, (const uint32_t*)ctx->starts.p,
                             (const uint32_t*)ctx->idx.p, (const float*)ctx->w.p, (float4*)ctx->cluster_rad.p, ctl,
-                            it, &l, 1);
+                            it, &l, 1, ctx->sell_ready ? &ctx->sellm : nullptr);
         ctx->launches += (uint64_t)l;
     }
     ctx->launches += (uint64_t)launch_grid_refresh(ctx->st, (const uint32_t*)ctx->gitems.p, s.irr, n,

@@ -159,17 +159,129 @@ void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_
         k_light_surfels<NoCount><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, nullptr, terms);
 }
 
+// solve.rs:76-102 over the sliced-ELL copy: one thread per sorted position
+// (its warp is its slice), the row's links read 4 at a time as 128-bit loads
+// from the interleaved layout (a warp's loads are one contiguous 512-byte
+// block) and added in CSR order, exactly as k_jacobi; a lane stops at its own
+// row's length, so padding is never read. Outputs go to the original row.
+__global__ void __launch_bounds__(kJacBlock) k_jacobi_sell(float4* direct, float4* albedo, float4* irr_out,
+                                                            float4* rad, uint32_t n, SellMatrix m,
+                                                            const float4* __restrict__ crad, SolveCtl* ctl) {
+    if (ctl->done) return;
+    float dmax = 0.0f;
+    for (uint32_t sp = blockIdx.x * blockDim.x + threadIdx.x; sp < n; sp += gridDim.x * blockDim.x) {
+        const uint32_t row = m.perm[sp], len = m.len[sp];
+        const uint32_t* ip = m.idx + m.slice_off[sp >> 5] + (sp & 31u) * 4u;
+        const float* wp = m.w + m.slice_off[sp >> 5] + (sp & 31u) * 4u;
+        V irr{0.0f, 0.0f, 0.0f};
+        uint32_t j = 0;
+        for (; j + 8 <= len; j += 8, ip += 256, wp += 256) {
+            const uint4 i0 = __ldg(reinterpret_cast<const uint4*>(ip));
+            const uint4 i1 = __ldg(reinterpret_cast<const uint4*>(ip + 128));
+            const float4 w0 = __ldg(reinterpret_cast<const float4*>(wp));
+            const float4 w1 = __ldg(reinterpret_cast<const float4*>(wp + 128));
+            const float4 c0 = __ldg(&crad[i0.x]), c1 = __ldg(&crad[i0.y]), c2 = __ldg(&crad[i0.z]),
+                         c3 = __ldg(&crad[i0.w]), c4 = __ldg(&crad[i1.x]), c5 = __ldg(&crad[i1.y]),
+                         c6 = __ldg(&crad[i1.z]), c7 = __ldg(&crad[i1.w]);
+            irr = irr + mk4(c0) * w0.x;
+            irr = irr + mk4(c1) * w0.y;
+            irr = irr + mk4(c2) * w0.z;
+            irr = irr + mk4(c3) * w0.w;
+            irr = irr + mk4(c4) * w1.x;
+            irr = irr + mk4(c5) * w1.y;
+            irr = irr + mk4(c6) * w1.z;
+            irr = irr + mk4(c7) * w1.w;
+        }
+        if (j < len) {
+            const uint4 i0 = __ldg(reinterpret_cast<const uint4*>(ip));
+            const float4 w0 = __ldg(reinterpret_cast<const float4*>(wp));
+            const uint32_t ia[4] = {i0.x, i0.y, i0.z, i0.w};
+            const float wa[4] = {w0.x, w0.y, w0.z, w0.w};
+            const uint32_t r4 = len - j < 4u ? len - j : 4u;
+            for (uint32_t t = 0; t < r4; ++t) irr = irr + mk4(__ldg(&crad[ia[t]])) * wa[t];
+            j += r4;
+            if (j < len) {
+                ip += 128;
+                wp += 128;
+                const uint4 i1 = __ldg(reinterpret_cast<const uint4*>(ip));
+                const float4 w1 = __ldg(reinterpret_cast<const float4*>(wp));
+                const uint32_t ib[4] = {i1.x, i1.y, i1.z, i1.w};
+                const float wb[4] = {w1.x, w1.y, w1.z, w1.w};
+                for (uint32_t t = 0; t < len - j; ++t) irr = irr + mk4(__ldg(&crad[ib[t]])) * wb[t];
+            }
+        }
+        V nr = mk4(direct[row]) + mk4(albedo[row]) * irr;
+        V diff = vabs(nr - mk4(rad[row]));
+        float d = fmaxf(diff.x, fmaxf(diff.y, diff.z));
+        irr_out[row] = f4(irr, 0.0f);
+        rad[row] = f4(nr, 0.0f);
+        if (!isnan(d)) dmax = fmaxf(dmax, d);
+    }
+    for (int o = 16; o >= 1; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
+    if ((threadIdx.x & 31) == 0 && dmax > 0.0f) atomicMax(&ctl->residual_bits, __float_as_uint(dmax));
+}
+
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
                          const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches,
-                         int no_exit) {
+                         int no_exit, const SellMatrix* sell) {
     k_cluster_agg<<<nc < 4096u ? nc : 4096u, kAggBlock, 0, st>>>(s.rad, s.p, cp, crange, members, nc, cluster_rad,
                                                                    ctl);
-    const int vec = (((uintptr_t)idx | (uintptr_t)w) & 15u) == 0 ? 1 : 0;
-    k_jacobi<<<grid_for(n, kJacBlock), kJacBlock, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, starts, idx, w,
-                                                          cluster_rad, ctl, vec);
+    if (sell && sell->perm) {
+        k_jacobi_sell<<<grid_for(n, kJacBlock), kJacBlock, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, *sell,
+                                                                   cluster_rad, ctl);
+    } else {
+        const int vec = (((uintptr_t)idx | (uintptr_t)w) & 15u) == 0 ? 1 : 0;
+        k_jacobi<<<grid_for(n, kJacBlock), kJacBlock, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, starts, idx, w,
+                                                              cluster_rad, ctl, vec);
+    }
     k_bounce_end<<<1, 1, 0, st>>>(ctl, it, no_exit);
     *launches += 3;
+}
+
+// ------------------------------------------------- sliced-ELL assembly ---
+__global__ void k_sell_lens(const uint32_t* starts, uint32_t n, uint32_t* lens, uint32_t* rows) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        lens[i] = starts[i + 1] - starts[i];
+        rows[i] = i;
+    }
+}
+
+// Entries of slice k: 32 lanes x its longest row rounded up to 4 (rows are
+// sorted by length, so that is the slice's first row).
+__global__ void k_sell_sizes(const uint32_t* sorted_len, uint32_t n, uint32_t* sizes) {
+    const uint32_t ns = (n + 31) / 32;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= ns; k += gridDim.x * blockDim.x)
+        sizes[k] = k < ns ? 32u * ((sorted_len[32 * k] + 3u) & ~3u) : 0u;
+}
+
+__global__ void k_sell_fill(const uint32_t* starts, const uint32_t* idx, const float* w, uint32_t n,
+                            const uint32_t* perm, const uint32_t* sorted_len, const uint32_t* slice_off,
+                            uint32_t* sidx, float* sw) {
+    for (uint32_t sp = blockIdx.x * blockDim.x + threadIdx.x; sp < n; sp += gridDim.x * blockDim.x) {
+        const uint32_t s0 = starts[perm[sp]], len = sorted_len[sp];
+        const uint32_t base = slice_off[sp >> 5] + (sp & 31u) * 4u;
+        for (uint32_t j = 0; j < len; ++j) {
+            const uint32_t q = base + (j >> 2) * 128u + (j & 3u);
+            sidx[q] = idx[s0 + j];
+            sw[q] = w[s0 + j];
+        }
+    }
+}
+
+int launch_sell_lens(cudaStream_t st, const uint32_t* starts, uint32_t n, uint32_t* lens, uint32_t* rows) {
+    k_sell_lens<<<grid_for(n, 256), 256, 0, st>>>(starts, n, lens, rows);
+    return 1;
+}
+int launch_sell_sizes(cudaStream_t st, const uint32_t* sorted_len, uint32_t n, uint32_t* sizes) {
+    k_sell_sizes<<<grid_for((unsigned long long)(n + 31) / 32 + 1, 256), 256, 0, st>>>(sorted_len, n, sizes);
+    return 1;
+}
+int launch_sell_fill(cudaStream_t st, const uint32_t* starts, const uint32_t* idx, const float* w, uint32_t n,
+                     const uint32_t* perm, const uint32_t* sorted_len, const uint32_t* slice_off, uint32_t* sidx,
+                     float* sw) {
+    k_sell_fill<<<grid_for(n, 256), 256, 0, st>>>(starts, idx, w, n, perm, sorted_len, slice_off, sidx, sw);
+    return 1;
 }
 
 void configure_solve_kernels(int max_dyn_smem) {

@@ -134,10 +134,30 @@ struct SolveCtl {
 // the light is skipped), for the differentiable relight.
 void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_t n, unsigned long long* evals,
                           uint32_t* status, unsigned long long* counts = nullptr, float* terms = nullptr);
+// The transfer in sliced-ELL form (k_solve.cu): rows sorted by link count
+// (descending, stable), slices of 32 consecutive sorted rows, each slice's
+// links stored as [link / 4][lane][link % 4] so that a warp's 32 rows read
+// one contiguous 512-byte block per 4 links. Every row keeps its links in
+// CSR order. perm == nullptr means "use the CSR arrays".
+struct SellMatrix {
+    const uint32_t* perm;       // sorted position -> row
+    const uint32_t* len;        // sorted position -> link count
+    const uint32_t* slice_off;  // per slice: first entry (multiple of 128)
+    const uint32_t* idx;
+    const float* w;
+};
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
                          const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches,
-                         int no_exit = 0);
+                         int no_exit = 0, const SellMatrix* sell = nullptr);
+// Sliced-ELL construction: row link counts (keys) with the identity (vals);
+// after a stable descending sort of (keys, vals), the slice sizes, then the
+// interleaved copy of idx and w.
+int launch_sell_lens(cudaStream_t st, const uint32_t* starts, uint32_t n, uint32_t* lens, uint32_t* rows);
+int launch_sell_sizes(cudaStream_t st, const uint32_t* sorted_len, uint32_t n, uint32_t* sizes);
+int launch_sell_fill(cudaStream_t st, const uint32_t* starts, const uint32_t* idx, const float* w, uint32_t n,
+                     const uint32_t* perm, const uint32_t* sorted_len, const uint32_t* slice_off, uint32_t* sidx,
+                     float* sw);
 
 // ---- batched relighting (solve.rs:47-108 over R right-hand sides) ----
 int launch_batch_init(cudaStream_t st, const float* E, uint32_t n, uint32_t R, float4* direct, float4* rad,
