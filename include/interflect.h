@@ -175,7 +175,8 @@ int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene);
 /* ----------------------------------------------------------- surfels --- */
 
 /* Replaces surfel::generate (src/surfel.rs:147-255): Halton seeds projected
- * onto the SDF on the GPU, then Poisson-thinned in seed order on the host.
+ * onto the SDF and Poisson-thinned on the GPU, with the reference's
+ * seed-order acceptance (the same surfels in the same order).
  * `placed` receives the surfel count. */
 int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* placed);
 

@@ -7,7 +7,7 @@ namespace ifx {
 // Newton projection onto the zero level set (at most 10 steps), then the
 // on-surface and in-bounds tests. Writes the projected point with w = 1 if
 // the seed survives, w = 0 otherwise. The Poisson-disc thinning that follows
-// is sequential in seed order and runs on the host.
+// (below) keeps the reference's seed-order semantics.
 __global__ void __launch_bounds__(128) k_gen_project(BlobRef blob, SceneConsts sc, uint32_t seed0,
                                                       uint32_t count, float eps, float4* out, uint32_t* status) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
@@ -245,25 +245,47 @@ __global__ void k_seg_starts(const unsigned long long* s, const uint32_t* head_s
     }
 }
 
-// formfactor.rs:119-145: sequential area-weighted sums in member order.
-__global__ void k_cluster_reduce(const uint32_t* seg_start, const uint32_t* members, uint32_t nseg,
-                                 const float4* sp, const float4* sn, float4* cp, float4* cn, uint32_t* valid) {
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nseg; c += gridDim.x * blockDim.x) {
+// formfactor.rs:119-145: sequential area-weighted sums in member order. One
+// CTA per segment: the threads stage each member's p * area, n * area and
+// area (each product rounds the same whoever forms it) in shared memory, a
+// chunk at a time, and thread 0 adds them in member order.
+static constexpr int kRedBlock = 128;
+__global__ void __launch_bounds__(kRedBlock) k_cluster_reduce(const uint32_t* seg_start, const uint32_t* members,
+                                                               uint32_t nseg, const float4* sp, const float4* sn,
+                                                               float4* cp, float4* cn, uint32_t* valid) {
+    __shared__ float4 bp[kRedBlock], bn[kRedBlock];
+    for (uint32_t c = blockIdx.x; c < nseg; c += gridDim.x) {
+        const uint32_t s0 = seg_start[c], s1 = seg_start[c + 1];
         V p{0.0f, 0.0f, 0.0f}, n{0.0f, 0.0f, 0.0f};
         float area = 0.0f;
-        for (uint32_t k = seg_start[c]; k < seg_start[c + 1]; ++k) {
-            uint32_t m = members[k];
-            float4 a = __ldg(&sp[m]);
-            float4 b = __ldg(&sn[m]);
-            p = p + mk4(a) * a.w;
-            n = n + mk4(b) * a.w;
-            area += a.w;
+        for (uint32_t k0 = s0; k0 < s1; k0 += kRedBlock) {
+            const uint32_t k = k0 + threadIdx.x;
+            if (k < s1) {
+                const uint32_t m = members[k];
+                const float4 a = __ldg(&sp[m]);
+                const float4 b = __ldg(&sn[m]);
+                bp[threadIdx.x] = make_float4(a.x * a.w, a.y * a.w, a.z * a.w, a.w);
+                bn[threadIdx.x] = make_float4(b.x * a.w, b.y * a.w, b.z * a.w, 0.0f);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const uint32_t cnt = min((uint32_t)kRedBlock, s1 - k0);
+                for (uint32_t j = 0; j < cnt; ++j) {
+                    const float4 u = bp[j], v = bn[j];
+                    p = p + V{u.x, u.y, u.z};
+                    n = n + V{v.x, v.y, v.z};
+                    area += u.w;
+                }
+            }
+            __syncthreads();
         }
-        bool ok = area > 1e-12f;
-        valid[c] = ok ? 1u : 0u;
-        V nn = dot(n, n) > 1e-12f ? nrm(n) : V{0.0f, 1.0f, 0.0f};
-        cp[c] = f4(p / area, area);
-        cn[c] = f4(nn, sqrtf(area / kPiF));
+        if (threadIdx.x == 0) {
+            bool ok = area > 1e-12f;
+            valid[c] = ok ? 1u : 0u;
+            V nn = dot(n, n) > 1e-12f ? nrm(n) : V{0.0f, 1.0f, 0.0f};
+            cp[c] = f4(p / area, area);
+            cn[c] = f4(nn, sqrtf(area / kPiF));
+        }
     }
 }
 
@@ -292,7 +314,8 @@ void launch_seg_starts(cudaStream_t st, const unsigned long long* sorted, const 
 }
 void launch_cluster_reduce(cudaStream_t st, const uint32_t* seg_start, const uint32_t* members, uint32_t nseg,
                            const float4* sp, const float4* sn, float4* cp, float4* cn, uint32_t* valid) {
-    k_cluster_reduce<<<grid_for(nseg, 64), 64, 0, st>>>(seg_start, members, nseg, sp, sn, cp, cn, valid);
+    k_cluster_reduce<<<nseg < 65535u ? (nseg ? nseg : 1u) : 65535u, kRedBlock, 0, st>>>(seg_start, members, nseg, sp,
+                                                                                       sn, cp, cn, valid);
 }
 void launch_cluster_compact(cudaStream_t st, const uint32_t* valid, const uint32_t* valid_scan, uint32_t nseg,
                             const uint32_t* seg_start, const float4* cp_in, const float4* cn_in, float4* cp,
