@@ -30,6 +30,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libinterflect_b200.so")
 CLI_PATH = os.path.join(_HERE, "bin", "interflect")
+COMPARE_PATH = os.path.join(_HERE, "bin", "compare")
 
 IFX_OK, IFX_ERR_INVALID, IFX_ERR_PARSE, IFX_ERR_CUDA, IFX_ERR_NOMEM, IFX_ERR_LIMIT, IFX_ERR_TIMEOUT = range(7)
 MODES = {"beauty": 0, "direct": 1, "indirect": 2, "normals": 3, "depth": 4, "steps": 5}

@@ -3,6 +3,7 @@
 Outputs
   interflect_b200/lib/libinterflect_b200.so   CUDA kernels + C ABI (sm_100a)
   interflect_b200/bin/interflect              the `interflect render` CLI
+  interflect_b200/bin/compare                 the image comparison tool (host only)
 
 The kernels are compiled with --fmad=false and IEEE division and square
 root so that every f32 expression rounds exactly as the reference's unfused
@@ -24,6 +25,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "lib", "libinterflect_b200.so")
 CLI = os.path.join(HERE, "bin", "interflect")
+COMPARE = os.path.join(HERE, "bin", "compare")
 
 CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "k_batch.cu", "k_diff.cu", "k_multi.cu",
               "capi.cu", "noalloc.cu"]
@@ -91,6 +93,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, png_src, LIB] + hdrs)):
         _run(["g++", *CXX_FLAGS, "-I", os.path.join(ROOT, "include"), cli_src, png_src, "-o", CLI,
               "-L", os.path.dirname(LIB), "-linterflect_b200", "-Wl,-rpath,$ORIGIN/../lib", "-lz"], verbose)
+    cmp_src = os.path.join(CSRC, "compare.cpp")
+    if os.path.exists(cmp_src) and (force or _stale(COMPARE, [cmp_src, png_src])):
+        _run(["g++", *CXX_FLAGS, cmp_src, png_src, "-o", COMPARE, "-lz"], verbose)
     return LIB
 
 
