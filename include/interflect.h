@@ -42,8 +42,8 @@ extern "C" {
 #define IFX_ERR_LIMIT 5    /* a size limit was exceeded */
 #define IFX_ERR_TIMEOUT 6  /* a bounded device-side wait expired */
 
-/* Render modes: main.rs:25-39 (the path-traced `reference` mode is not part
- * of this library). */
+/* Render modes: main.rs:25-39 (the path-traced `reference` mode has its own
+ * entry point, ifx_render_reference). */
 #define IFX_MODE_BEAUTY 0
 #define IFX_MODE_DIRECT 1
 #define IFX_MODE_INDIRECT 2
@@ -383,6 +383,21 @@ int ifx_multiscene_run(ifx_multiscene* ms, float* ms_out);
  * (w*h*3 u8) and solve statistics; each nullable. */
 int ifx_multiscene_download(ifx_multiscene* ms, int index, float* out_linear, uint8_t* out_srgb,
                             ifx_solve_stats* stats);
+
+/* ----------------------------------------------------- reference mode --- */
+
+/* Replaces render_frame in --mode reference (src/main.rs:249-259 with
+ * src/reference.rs:24-137): the brute-force path tracer the reference ships
+ * as ground truth, spp paths per pixel from a PCG32 stream seeded with
+ * (y << 32) | x, next-event estimation against the quad lights, cosine
+ * bounces, Russian roulette, at most 12 vertices. Tone-mapped film and
+ * encode as render_frame; out_linear and out_srgb are nullable. The first
+ * call on a context also tabulates the libm sine and cosine of the sampler's
+ * 2^24 azimuths on the host (128 MiB on the device), so that every pixel
+ * equals the CPU path's. Sphere lights (an extension) are not sampled, as in
+ * the reference, whose path tracer only knows quad lights. */
+int ifx_render_reference(ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, uint32_t h, uint32_t spp, float exposure,
+                         float* out_linear, uint8_t* out_srgb);
 
 #ifdef __cplusplus
 }

@@ -49,7 +49,7 @@ EXPORTS = (
     "ifx_diff_forward", "ifx_diff_backward",
     "ifx_multiscene_create", "ifx_multiscene_destroy", "ifx_multiscene_last_error", "ifx_multiscene_add",
     "ifx_multiscene_build", "ifx_multiscene_run", "ifx_multiscene_download", "ifx_set_stage_limit",
-    "ifx_clusters_build",
+    "ifx_clusters_build", "ifx_render_reference",
 )
 NOALLOC_MAX_CLUSTERS = 16384
 KERNELS = {"visibility": 0, "closure": 1, "light": 2, "primary": 3, "shadow": 4, "reflect": 5, "shadow2": 6,
@@ -170,6 +170,7 @@ def lib() -> C.CDLL:
         "ifx_multiscene_download": (I, [P, I, P, P, C.POINTER(_SolveStats)]),
         "ifx_set_stage_limit": (I, [P, U32]),
         "ifx_clusters_build": (I, [P, I, C.POINTER(U64)]),
+        "ifx_render_reference": (I, [P, C.POINTER(_Camera), U32, U32, U32, F, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -471,6 +472,17 @@ class Context:
         self._check(lib().ifx_render_frame(self._h, C.byref(cam) if cam is not None else None, m, width, height,
                                            exposure, _ptr(lin), _ptr(s8), C.byref(e)), "render_frame")
         return lin, s8, e.value
+
+    def render_reference(self, width: int, height: int, spp: int = 512, cam=None, exposure: float | None = None,
+                         linear: bool = True, srgb: bool = True):
+        """--mode reference: the path tracer of reference.rs. Returns (linear | None, u8 | None)."""
+        if exposure is None:
+            exposure = self.scene.cfg.exposure if self.scene is not None else 1.0
+        lin = np.zeros((height, width, 3), np.float32) if linear else None
+        s8 = np.zeros((height, width, 3), np.uint8) if srgb else None
+        self._check(lib().ifx_render_reference(self._h, C.byref(cam) if cam is not None else None, width, height, spp,
+                                               exposure, _ptr(lin), _ptr(s8)), "render_reference")
+        return lin, s8
 
     def stats(self) -> dict:
         s = _Stats()

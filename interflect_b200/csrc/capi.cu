@@ -8,6 +8,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -96,6 +97,7 @@ struct ifx_ctx {
 
     // film
     DBuf film, out8;
+    DBuf path_sincos;  // (sinf, cosf) of the path tracer's 2^24 sampler angles
 
     // lights: current emission per light (float4), for the relight and adjoint
     DBuf lemit;
@@ -396,7 +398,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->dperm_alt, &ctx->draw, &ctx->gent, &ctx->gtstarts, &ctx->lrows, &ctx->fkey_alt,
                     &ctx->ft, &ctx->ftstarts, &ctx->cid, &ctx->hist, &ctx->dg, &ctx->h_t, &ctx->yv, &ctx->ebar,
                     &ctx->rhobar, &ctx->epart, &ctx->eout, &ctx->d3, &ctx->sell_len, &ctx->sell_perm, &ctx->sell_keys,
-                    &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w};
+                    &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w,
+                    &ctx->path_sincos};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -1393,6 +1396,76 @@ static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w
     ctx->stats.ms_shade_other = g[4] + g[5] + g[6];
     if (evals) *evals = e;
     if (saved) *saved = P;
+    return IFX_OK;
+}
+
+extern "C" int ifx_render_reference(ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
+                                    float exposure, float* out_linear, uint8_t* out_srgb) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (spp == 0 || spp > 1u << 20) return fail(ctx, IFX_ERR_LIMIT, "spp out of range (1..1048576)");
+    if (w == 0 || h == 0 || w > 16384u || h > 16384u || (uint64_t)w * h > 40000000ull)
+        return fail(ctx, IFX_ERR_LIMIT, "film size out of range");
+    CK(cudaSetDevice(ctx->device));
+    frame_changed(ctx);
+    // reference.rs:55 takes f32::sin/cos of TAU * u for u = k * 2^-24: the
+    // platform libm's values for every k, computed once per context.
+    const size_t nk = (size_t)1 << 24;
+    if (!ctx->path_sincos.p) {
+        std::vector<float2> tab(nk);
+        const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t)
+            pool.emplace_back([&, t]() {
+                for (size_t k = t; k < nk; k += nt) {
+                    const float phi = 6.28318530717958647692f * ((float)k * (1.0f / 16777216.0f));
+                    tab[k] = make_float2(std::sin(phi), std::cos(phi));
+                }
+            });
+        for (auto& th : pool) th.join();
+        ENSURE(ctx->path_sincos, nk * sizeof(float2));
+        CK(cudaMemcpy(ctx->path_sincos.p, tab.data(), nk * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+    const HScene& s = ctx->scene;
+    F3 pos = s.camera.pos, look = s.camera.look, up = s.camera.up;
+    float fov = s.camera.fov;
+    if (cam) {
+        pos = F3{cam->pos[0], cam->pos[1], cam->pos[2]};
+        look = F3{cam->look[0], cam->look[1], cam->look[2]};
+        up = F3{cam->up[0], cam->up[1], cam->up[2]};
+        fov = cam->fov;
+    }
+    CamBasis b = camera_basis(pos, look, up, fov, w, h);
+    ShadeParams P{};
+    P.blob = ctx->blobref;
+    memcpy(P.cam.origin, b.origin, 12);
+    memcpy(P.cam.fwd, b.fwd, 12);
+    memcpy(P.cam.right, b.right, 12);
+    memcpy(P.cam.up, b.up, 12);
+    P.cam.tan_half = b.tan_half;
+    P.cam.aspect = b.aspect;
+    P.w = w;
+    P.h = h;
+    P.tmax = ctx->sc.diag * 4.0f;  // main.rs:417
+    P.exposure = exposure;
+    P.tonemap = 1;  // main.rs:48: the reference mode is tone-mapped
+    P.srgb_t = (const float*)ctx->srgb_t.p;
+    P.status = (uint32_t*)ctx->status.p;
+    const size_t px = (size_t)w * h;
+    ENSURE(ctx->film, px * 12);
+    ENSURE(ctx->out8, px * 3);
+    P.film = (float*)ctx->film.p;
+    P.out8 = (uint8_t*)ctx->out8.p;
+    unsigned long long* cursor = (unsigned long long*)ctx->qcur.p;
+    CK(cudaMemsetAsync(cursor, 0, 8, ctx->st));
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    ctx->launches += (uint64_t)launch_path(ctx->st, P, spp, (const float2*)ctx->path_sincos.p, cursor);
+    CKL();
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    if (out_linear) CK(cudaMemcpyAsync(out_linear, ctx->film.p, px * 12, cudaMemcpyDeviceToHost, ctx->st));
+    if (out_srgb) CK(cudaMemcpyAsync(out_srgb, ctx->out8.p, px * 3, cudaMemcpyDeviceToHost, ctx->st));
+    int r = check_status(ctx);
+    if (r) return r;
+    CK(cudaEventElapsedTime(&ctx->stats.ms_shade, ctx->ev0, ctx->ev1));
     return IFX_OK;
 }
 

@@ -29,8 +29,8 @@ namespace {
             "    -t, --threads <N>      accepted for compatibility (GPU)\n"
             "    -w, --width <N>        override scene width\n"
             "    -h, --height <N>       override scene height\n"
-            "        --mode <MODE>      beauty | direct | indirect | normals | depth | steps\n"
-            "        --spp <N>          accepted for compatibility (no reference mode)\n"
+            "        --mode <MODE>      beauty | direct | indirect | normals | depth | steps | reference\n"
+            "        --spp <N>          samples/pixel for --mode reference   [default: 512]\n"
             "        --clusters <N>     transfer cluster grid resolution     [default: 8]\n"
             "        --surfels <N>      override surfel count\n"
             "        --bounces <N>      override bounce count\n"
@@ -87,7 +87,11 @@ int main(int argc, char** argv) {
     std::vector<std::string> a(argv + 1, argv + argc);
     if (a.size() < 2 || a[0] != "render") usage();
     std::string input = a[1], output = "out.png";
+    // `--mode reference` is the path tracer (reference.rs), which has its own
+    // entry point rather than an ifx_render_frame mode.
+    const int kModeReference = -1;
     int mode = IFX_MODE_BEAUTY, cluster_res = 8, device = 0;
+    uint32_t spp = 512;
     bool no_bvh = false;
     uint64_t turntable = 0, v = 0;
     bool have_w = false, have_h = false, have_s = false, have_b = false;
@@ -101,8 +105,12 @@ int main(int argc, char** argv) {
         if (f == "-o" || f == "--output") {
             output = need();
             i += 2;
-        } else if (f == "-t" || f == "--threads" || f == "--spp") {
+        } else if (f == "-t" || f == "--threads") {
             need();
+            i += 2;
+        } else if (f == "--spp") {
+            uint64_t v2 = 0;
+            spp = parse_u64(need(), v2) && v2 >= 1 && v2 <= (1u << 20) ? (uint32_t)v2 : 512u;  // main.rs:150-151; 0 and counts above 2^20 take the default
             i += 2;
         } else if (f == "-w" || f == "--width") {
             have_w = parse_u64(need(), ow) && ow <= 0xffffffffull;
@@ -133,10 +141,8 @@ int main(int argc, char** argv) {
             else if (m == "normals") mode = IFX_MODE_NORMALS;
             else if (m == "depth") mode = IFX_MODE_DEPTH;
             else if (m == "steps") mode = IFX_MODE_STEPS;
-            else if (m == "reference") {
-                fprintf(stderr, "error: --mode reference (the path tracer) is not part of this renderer\n");
-                return 1;
-            } else {
+            else if (m == "reference") mode = kModeReference;
+            else {
                 fprintf(stderr, "unknown mode `%s`\n", m.c_str());
                 usage();
             }
@@ -226,8 +232,6 @@ int main(int argc, char** argv) {
     const double gi_ms = ms_since(t_gi);
 
     std::vector<uint8_t> rgb((size_t)w * h * 3);
-    const bool tonemapped = mode <= IFX_MODE_INDIRECT;
-    (void)tonemapped;
     if (turntable > 0) {
         // main.rs:492-520: orbit the camera about its look point.
         const float tau = 6.28318530717958647692f;
@@ -241,8 +245,10 @@ int main(int argc, char** argv) {
             cam.pos[0] = info.camera.look[0] + (base[0] * co - base[2] * s);
             cam.pos[1] = info.camera.look[1] + base[1];
             cam.pos[2] = info.camera.look[2] + (base[0] * s + base[2] * co);
-            if (ifx_render_frame(ctx, &cam, mode, w, h, cfg.exposure, nullptr, rgb.data(), nullptr) != IFX_OK)
-                return fail_ctx(ctx, "render");
+            const int rc = mode == kModeReference
+                               ? ifx_render_reference(ctx, &cam, w, h, spp, cfg.exposure, nullptr, rgb.data())
+                               : ifx_render_frame(ctx, &cam, mode, w, h, cfg.exposure, nullptr, rgb.data(), nullptr);
+            if (rc != IFX_OK) return fail_ctx(ctx, "render");
             std::string stem = output;
             if (stem.size() >= 4 && stem.compare(stem.size() - 4, 4, ".png") == 0) stem.resize(stem.size() - 4);
             char name[64];
@@ -262,9 +268,11 @@ int main(int argc, char** argv) {
         return 0;
     }
     auto t0 = std::chrono::steady_clock::now();
-    uint64_t evals = 0;
-    if (ifx_render_frame(ctx, nullptr, mode, w, h, cfg.exposure, nullptr, rgb.data(), &evals) != IFX_OK)
-        return fail_ctx(ctx, "render");
+    uint64_t evals = 0;  // the path tracer counts no evaluations (main.rs:249-258)
+    const int rc = mode == kModeReference
+                       ? ifx_render_reference(ctx, nullptr, w, h, spp, cfg.exposure, nullptr, rgb.data())
+                       : ifx_render_frame(ctx, nullptr, mode, w, h, cfg.exposure, nullptr, rgb.data(), &evals);
+    if (rc != IFX_OK) return fail_ctx(ctx, "render");
     double ms = ms_since(t0);
     double px = (double)w * (double)h;
     printf("  shade      %.0f ms   %.1fM sdf evals   %.0f evals/px\n", ms, (double)evals / 1e6, (double)evals / px);

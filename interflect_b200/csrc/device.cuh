@@ -981,8 +981,9 @@ __device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V alb
 // shade.rs:168-181 with trace.rs:128-148 (and sphere-light entry points).
 // `which` (nullable) receives the index of the light picked (quad lights,
 // then sphere lights).
+// quads_only: the quad lights alone (reference.rs passes &sc.lights).
 __device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, float tmax, V& emit,
-                                            int* which = nullptr) {
+                                            int* which = nullptr, bool quads_only = false) {
     bool found = false;
     float best = 0.0f;
     for (int li = 0; li < sv.n_lights; ++li) {
@@ -1004,6 +1005,7 @@ __device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, flo
             if (which) *which = li;
         }
     }
+    if (quads_only) return found;
     for (int li = 0; li < sv.n_slights; ++li) {
         const DSphereLight& L = sv.slights[li];
         V oc = ro - V{L.c[0], L.c[1], L.c[2]};

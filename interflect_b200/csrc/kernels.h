@@ -309,12 +309,18 @@ void configure_transfer_kernels(int max_dyn_smem);
 void configure_solve_kernels(int max_dyn_smem);
 void configure_shade_kernels(int max_dyn_smem);
 void configure_diff_kernels(int max_dyn_smem);
+void configure_path_kernels(int max_dyn_smem);
+// The path-traced reference mode (k_path.cu): p.film / p.out8 receive the
+// frame; sincos holds (sinf, cosf) of the 2^24 sampler angles.
+int launch_path(cudaStream_t st, const ShadeParams& p, uint32_t spp, const float2* sincos,
+                unsigned long long* cursor);
 inline void configure_kernels(int max_dyn_smem) {
     configure_surfel_kernels(max_dyn_smem);
     configure_transfer_kernels(max_dyn_smem);
     configure_solve_kernels(max_dyn_smem);
     configure_shade_kernels(max_dyn_smem);
     configure_diff_kernels(max_dyn_smem);
+    configure_path_kernels(max_dyn_smem);
 }
 
 }  // namespace ifx

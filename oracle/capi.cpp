@@ -25,6 +25,7 @@ struct orc_ctx {
     int threads = 1;
     std::string err;
     SolveStats stats{0, 0.0f};
+    uint32_t spp = 512;  // samples per pixel of the path-traced reference mode
     DiffModel* diff = nullptr;
     ~orc_ctx() { diff_free(diff); }
 };
@@ -355,8 +356,10 @@ int64_t orc_render(orc_ctx* c, int mode, uint32_t w, uint32_t h, const float* po
     c->fw = w;
     c->fh = h;
     return (int64_t)render_frame(s, cam, mode, needs_gi && c->has_grid ? &gi : nullptr, tmax, w, h, c->film,
-                                 c->threads, y0, y1);
+                                 c->threads, y0, y1, c->spp);
 }
+
+void orc_set_spp(orc_ctx* c, uint32_t spp) { c->spp = spp < 1 ? 1 : spp; }
 
 int orc_get_film(orc_ctx* c, float* rgb) {
     put3(rgb, c->film);

@@ -401,7 +401,7 @@ static bool intersect_sphere(V3 c, float r, V3 ro, V3 rd, float& t_out) {
 }
 
 // shade.rs:168-181
-bool emitter_hit(const Scene& sc, V3 ro, V3 rd, float tmax, float& t_best, V3& emit) {
+bool emitter_hit(const Scene& sc, V3 ro, V3 rd, float tmax, float& t_best, V3& emit, bool quads_only) {
     bool found = false;
     for (const QuadLight& l : sc.lights) {
         float t;
@@ -413,6 +413,7 @@ bool emitter_hit(const Scene& sc, V3 ro, V3 rd, float tmax, float& t_best, V3& e
             }
         }
     }
+    if (quads_only) return found;
     for (const SphereLight& l : sc.sphere_lights) {  // [ext]
         float t;
         if (intersect_sphere(l.c, l.r, ro, rd, t)) {

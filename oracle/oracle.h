@@ -165,7 +165,9 @@ V3 f0_of(const Material& m);                 // shade.rs:36-38
 V3 diffuse_albedo(const Material& m);        // shade.rs:41-43
 V3 direct(const Scene& sc, V3 p, V3 n, V3 v, const Material& m, uint32_t& steps);  // shade.rs:50-125
 V3 direct_diffuse(const Scene& sc, V3 p, V3 n, V3 albedo, uint32_t& steps);      // shade.rs:133-164
-bool emitter_hit(const Scene& sc, V3 ro, V3 rd, float tmax, float& t, V3& emit);  // shade.rs:168-181
+// shade.rs:168-181; quads_only: the quad lights alone, as reference.rs passes
+// &sc.lights (the sphere-light extension is not part of the path tracer).
+bool emitter_hit(const Scene& sc, V3 ro, V3 rd, float tmax, float& t, V3& emit, bool quads_only = false);
 // The same test returning the index of the light it picks (quad lights, then
 // sphere lights), -1 when none.
 int emitter_index(const Scene& sc, V3 ro, V3 rd, float tmax);
@@ -228,7 +230,9 @@ SolveStats solve(Surfels& s, const Transfer& t, uint32_t max_bounces, int thread
                  bool no_exit = false);  // solve.rs:47-108
 
 // ----------------------------------------------------------------- main.rs --
-enum Mode : int32_t { M_BEAUTY = 0, M_DIRECT = 1, M_INDIRECT = 2, M_NORMALS = 3, M_DEPTH = 4, M_STEPS = 5 };
+enum Mode : int32_t {
+    M_BEAUTY = 0, M_DIRECT = 1, M_INDIRECT = 2, M_NORMALS = 3, M_DEPTH = 4, M_STEPS = 5, M_REFERENCE = 6
+};
 
 struct Cam {  // main.rs:188-218
     V3 origin, fwd, right, up;
@@ -246,9 +250,19 @@ struct Gi {  // main.rs:222-226
 // main.rs:229-367 (the path-traced reference mode is not part of this path).
 // `rows` restricts shading to a subset [y0, y1) of rows when y1 > y0; the
 // evaluation count of only those rows is returned.
+// M_REFERENCE is the brute-force path tracer of reference.rs with `spp`
+// samples per pixel (main.rs:249-259).
 uint64_t render_frame(const Scene& sc, const Cam& cam, int32_t mode, const Gi* gi, float tmax,
                       uint32_t w, uint32_t h, std::vector<V3>& film, int threads,
-                      uint32_t y0 = 0, uint32_t y1 = 0);
+                      uint32_t y0 = 0, uint32_t y1 = 0, uint32_t spp = 512);
+
+// reference.rs:24-46 (PCG32) and :61-137 (one path).
+struct Pcg {
+    uint64_t s;
+    explicit Pcg(uint64_t seed);
+    float next_f32();
+};
+V3 path(const Scene& sc, V3 ro, V3 rd, float tmax, uint32_t max_depth, Pcg& rng);
 
 // film.rs:8-61
 V3 aces(V3 x);

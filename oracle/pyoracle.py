@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 RENDER_BIN = os.path.join(HERE, "_build", "oracle_render")
 
-MODES = {"beauty": 0, "direct": 1, "indirect": 2, "normals": 3, "depth": 4, "steps": 5}
+MODES = {"beauty": 0, "direct": 1, "indirect": 2, "normals": 3, "depth": 4, "steps": 5, "reference": 6}
 
 _lib = None
 
@@ -52,7 +52,7 @@ def lib() -> C.CDLL:
             "orc_camera": (I, [P, P, P, F, U32, U32, P]),
             "orc_render": (I64, [P, I, U32, U32, P, P, U32, U32]), "orc_get_film": (I, [P, P]),
             "orc_encode": (I, [P, F, I, P]), "orc_counters": (None, [I, I, P]),
-            "orc_solve_ex": (I, [P, U32, I, P, P]), "orc_set_emission": (I, [P, I64, P]),
+            "orc_solve_ex": (I, [P, U32, I, P, P]), "orc_set_spp": (None, [P, U32]), "orc_set_emission": (I, [P, I64, P]),
             "orc_get_emission": (I, [P, P]), "orc_diff_build": (I, [P, U32, U32, P]),
             "orc_diff_loss": (C.c_double, [P, P, P, I, P, P]), "orc_diff_grad": (C.c_double, [P, P, P, I, P, P, P]),
         }
@@ -263,9 +263,11 @@ class Oracle:
         lib().orc_gather(self.h, len(p), _p(p), _p(n), _p(out))
         return out
 
-    def render(self, width: int, height: int, mode="beauty", pos=None, look=None, rows=None):
-        """Linear film (H x W x 3) and the SDF evaluation count. `rows` = (y0, y1) shades only those rows."""
+    def render(self, width: int, height: int, mode="beauty", pos=None, look=None, rows=None, spp: int = 512):
+        """Linear film (H x W x 3) and the SDF evaluation count. `rows` = (y0, y1) shades only those rows;
+        `spp` is the path tracer's samples per pixel (mode "reference")."""
         m = MODES[mode] if isinstance(mode, str) else int(mode)
+        lib().orc_set_spp(self.h, spp)
         y0, y1 = rows if rows else (0, 0)
         ev = lib().orc_render(self.h, m, width, height, _p(None if pos is None else f32(pos)),
                               _p(None if look is None else f32(look)), y0, y1)

@@ -30,16 +30,95 @@ V3 Cam::ray(uint32_t x, uint32_t y, uint32_t w, uint32_t h) const {
 
 static const V3 SKY(0.02f, 0.03f, 0.05f);
 
-// One pixel of main.rs:247-361 (non-reference modes).
+// reference.rs:31-46
+Pcg::Pcg(uint64_t seed) : s(seed * 6364136223846793005ull + 1ull) {}
+float Pcg::next_f32() {
+    s = s * 6364136223846793005ull + 1442695040888963407ull;
+    const uint64_t x = ((s >> 18) ^ s) >> 27;
+    const uint32_t rot = (uint32_t)(s >> 59);
+    const uint32_t v0 = (uint32_t)x;
+    const uint32_t v = (v0 >> rot) | (v0 << ((32u - rot) & 31u));
+    return (float)(v >> 8) * (1.0f / 16777216.0f);
+}
+
+// reference.rs:48-57
+static V3 cosine_hemisphere(V3 n, Pcg& rng) {
+    V3 t, b;
+    frame(n, t, b);
+    const float u1 = rng.next_f32();
+    const float u2 = rng.next_f32();
+    const float r = std::sqrt(u1);
+    const float phi = TAU_F * u2;
+    return normalize(t * (r * std::cos(phi)) + b * (r * std::sin(phi)) + n * std::sqrt(fmaxr(1.0f - u1, 0.0f)));
+}
+
+// reference.rs:61-137
+V3 path(const Scene& sc, V3 ro, V3 rd, float tmax, uint32_t max_depth, Pcg& rng) {
+    V3 radiance(0.0f, 0.0f, 0.0f), throughput(1.0f, 1.0f, 1.0f);
+    V3 origin = ro, dir = rd;
+    for (uint32_t depth = 0; depth < max_depth; ++depth) {
+        Hit h;
+        uint32_t steps;
+        const bool hit = trace(sc, origin, dir, 1e-3f, tmax, h, steps);
+        const float surf_t = hit ? h.t : 3.40282347e38f;
+        float et;
+        V3 e;
+        if (emitter_hit(sc, origin, dir, fminr(surf_t, tmax), et, e, true)) {
+            if (depth == 0) radiance += throughput * e;
+            break;
+        }
+        if (!hit) break;
+        const Material m = sc.material(h.mat);
+        const V3 albedo = diffuse_albedo(m);
+        radiance += throughput * m.emissive;
+        for (const QuadLight& light : sc.lights) {
+            const V3 e1 = light.verts[1] - light.verts[0];
+            const V3 e2 = light.verts[3] - light.verts[0];
+            const float r1 = rng.next_f32();
+            const float r2 = rng.next_f32();
+            const V3 lp = light.verts[0] + e1 * r1 + e2 * r2;
+            const V3 to = lp - h.p;
+            const float dist2 = length_squared(to);
+            if (dist2 < 1e-9f) continue;
+            const float dist = std::sqrt(dist2);
+            const V3 l = to / dist;
+            const float cos_s = dot(h.n, l);
+            const float cos_l = dot(light.normal(), -l);
+            if (cos_s <= 0.0f || cos_l <= 0.0f) continue;
+            Hit occ;
+            uint32_t s2;
+            if (trace(sc, h.p + h.n * 1e-3f, l, 1e-3f, dist - 1e-2f, occ, s2)) continue;
+            const float pdf = dist2 / (cos_l * light.area());
+            radiance += throughput * albedo * light.emit * (cos_s / (PI_F * pdf));
+        }
+        throughput = throughput * albedo;
+        dir = cosine_hemisphere(h.n, rng);
+        origin = h.p + h.n * 1e-3f;
+        if (depth >= 3) {
+            const float q = clampf(max_element(throughput), 0.05f, 0.95f);
+            if (rng.next_f32() > q) break;
+            throughput = throughput / q;
+        }
+    }
+    return radiance;
+}
+
+// One pixel of main.rs:247-361.
 static V3 shade_pixel(const Scene& sc, const Cam& cam, int32_t mode, const Gi* gi, float tmax, uint32_t x,
-                      uint32_t y, uint32_t w, uint32_t h, uint64_t& local) {
+                      uint32_t y, uint32_t w, uint32_t h, uint64_t& local, uint32_t spp) {
     V3 rd = cam.ray(x, y, w, h);
+    if (mode == M_REFERENCE) {  // main.rs:249-259
+        Pcg rng(((uint64_t)y << 32) | (uint64_t)x);
+        V3 acc(0.0f, 0.0f, 0.0f);
+        for (uint32_t i = 0; i < spp; ++i) acc += path(sc, cam.origin, rd, tmax, 12, rng);
+        return acc / (float)spp;
+    }
     Hit hh;
     uint32_t steps;
     bool hit = trace(sc, cam.origin, rd, 1e-3f, tmax, hh, steps);
     local += steps;
     float surf_t = hit ? hh.t : 3.40282347e38f;
-    bool tonemapped = (mode == M_BEAUTY || mode == M_DIRECT || mode == M_INDIRECT);
+    bool tonemapped = (mode == M_BEAUTY || mode == M_DIRECT || mode == M_INDIRECT || mode == M_REFERENCE);
     float et;
     V3 e;
     if (emitter_hit(sc, cam.origin, rd, fminr(surf_t, tmax), et, e)) return tonemapped ? e : V3::splat(0.9f);
@@ -102,7 +181,7 @@ static V3 shade_pixel(const Scene& sc, const Cam& cam, int32_t mode, const Gi* g
 
 // main.rs:229-367
 uint64_t render_frame(const Scene& sc, const Cam& cam, int32_t mode, const Gi* gi, float tmax, uint32_t w,
-                      uint32_t h, std::vector<V3>& film, int threads, uint32_t y0, uint32_t y1) {
+                      uint32_t h, std::vector<V3>& film, int threads, uint32_t y0, uint32_t y1, uint32_t spp) {
     film.assign((size_t)w * (size_t)h, V3());
     if (y1 <= y0) {
         y0 = 0;
@@ -114,7 +193,7 @@ uint64_t render_frame(const Scene& sc, const Cam& cam, int32_t mode, const Gi* g
         uint32_t y = y0 + r;
         uint64_t local = 0;
         for (uint32_t x = 0; x < w; ++x)
-            film[(size_t)y * w + x] = shade_pixel(sc, cam, mode, gi, tmax, x, y, w, h, local);
+            film[(size_t)y * w + x] = shade_pixel(sc, cam, mode, gi, tmax, x, y, w, h, local, spp);
         row_evals[r] = local;
     };
     if (threads <= 1) {
