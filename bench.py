@@ -48,11 +48,16 @@ WORKLOADS = {
     "solve_hbm": ("interflect_b200/scenes/c3_stress.rad",
                   "Jacobi solve alone on a stress-sized transfer: the stress scene's 1M surfels and clusters with "
                   "a synthetic CSR of 109 links per row (109M links), 24 bounces max; the HBM-bound stage"),
+    "pathtrace": ("tests/golden/scenes/bench_cornell.rad",
+                  "the path-traced ground truth of the accuracy benchmark: Lambertian Cornell box, 300x300, 512 "
+                  "samples per pixel (bench.sh defaults)"),
     "c5_diff": ("interflect_b200/scenes/c5_cornell_fill.rad",
                 "Cornell box 512x512 with a second (fill) light, 20k surfels, 12 fixed bounces; L2 loss against a "
                 "target rendered from per-surfel albedo + N(0,0.05) clamped to [0.05,0.95]; gradient w.r.t. "
                 "per-surfel albedo and both light emissions"),
 }
+PT_METRIC = "path-traced samples per second (--mode reference, 12-vertex paths with next-event estimation)"
+PT_FILM, PT_SPP, PT_CPU_ROWS = 300, 512, 16
 DIFF_METRIC = "albedo+emission gradient ms (differentiable forward + adjoint) vs one forward frame"
 BATCH_METRIC = "relighting solves per second (256 right-hand sides on one transfer matrix)"
 METRIC = "SDF evaluations per second, one full frame (transfer + light + solve + grid + shade)"
@@ -706,9 +711,106 @@ def cpu_model() -> str:
     return "unknown"
 
 
+def run_pathtrace(args, world, rank, local) -> dict | None:
+    """The path tracer of `--mode reference` (reference.rs:61-137): one step
+    is one full film at 512 samples per pixel."""
+    import interflect_b200 as ifx
+    scene_path, desc = WORKLOADS[args.workload]
+    with open(os.path.join(ROOT, scene_path)) as f:
+        src = f.read()
+    scene = ifx.parse(src)
+    W = H = PT_FILM
+    if args.film:
+        W, H = (int(v) for v in args.film.lower().split("x"))
+    spp = PT_SPP
+    ctx = ifx.Context(local)
+    ctx.upload(scene)
+    ctx.set_work_counting(True)
+    ctx.reset_work()
+    ctx.render_reference(W, H, spp, linear=False, srgb=False)
+    counts, flops = ctx.work("path")
+    ctx.set_work_counting(False)
+    for _ in range(args.warmup):
+        ctx.render_reference(W, H, spp, linear=False, srgb=False)
+    flusher = L2Flusher(local)
+    barrier(world)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    launches0 = ctx.stats()["kernel_launches"]
+    total_ms, kms = 0.0, []
+    for _ in range(args.steps):
+        flusher.flush()
+        ctx.timer_start()
+        ctx.render_reference(W, H, spp, linear=False, srgb=False)
+        total_ms += ctx.timer_stop()
+        kms.append(ctx.stats()["ms_shade"])
+    launches = ctx.stats()["kernel_launches"] - launches0
+    clocks = sampler.stop() if sampler else None
+    barrier(world)
+    # End to end: the scene uploaded from host memory and the encoded image
+    # read back, every step.
+    e2e_ms, out8 = 0.0, None
+    for i in range(args.warmup + args.steps):
+        flusher.flush()
+        ctx.timer_start()
+        ctx.upload(scene)
+        _, out8 = ctx.render_reference(W, H, spp, linear=False, srgb=True)
+        ms = ctx.timer_stop()
+        if i >= args.warmup:
+            e2e_ms += ms
+    (t_max, e2e_max), _ = allreduce_max_sum([total_ms, e2e_ms], [0.0], world)
+    if rank != 0:
+        return None
+    samples = W * H * spp
+    value = samples * args.steps * world / (t_max / 1e3)
+    kavg = statistics.mean(kms)
+    peak, peak_src = fp32_peak_tflops(measured_peaks())
+    achieved = flops / (kavg / 1e3) / 1e12
+    line = {
+        "metric": PT_METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "scene": scene_path, "description": desc, "film": [W, H],
+                   "spp": spp, "max_depth": 12, "l2": "flushed (256 MB write) before every timed step",
+                   "parallelism": f"replicas x{world}"},
+        "kernel_ms": {"path": kavg},
+        "roofline": {"kernel": "path", "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None, "flops_per_launch": flops,
+                     "peak_source": f"fp32 CUDA-core peak from {peak_src}",
+                     "sdf_queries_per_launch": int(counts[11]), "march_steps_per_launch": int(counts[12])},
+        "e2e": {"value": samples * args.steps / (e2e_max / 1e3), "unit": "samples/s",
+                "h2d_bytes_per_step": len(src), "d2h_bytes_per_step": int(out8.nbytes),
+                "ms_per_step": e2e_max / args.steps},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = pathtrace_cpu(src, W, H, spp)
+    return line
+
+
+def pathtrace_cpu(src, W, H, spp, rows=PT_CPU_ROWS) -> dict:
+    """The oracle's path tracer on all host cores over the first `rows` rows."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Oracle
+    threads = os.cpu_count() or 1
+    o = Oracle(src, threads=threads)
+    rows = min(rows, H)
+    t0 = time.perf_counter()
+    o.render(W, H, "reference", rows=(0, rows), spp=spp)
+    dt = time.perf_counter() - t0
+    n = W * rows * spp
+    return {"value": n / dt, "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"rows 0..{rows} of the {W}x{H} film at {spp} spp ({n / 1e6:.2f}M samples in {dt:.2f} s)",
+            "cpu": cpu_model()}
+
+
 def run_reference(args, world, rank) -> dict | None:
     if rank != 0:
         return None
+    if args.workload == "pathtrace":
+        return run_reference_pathtrace(args, world)
     import interflect_b200  # noqa: F401  (scene parsing only)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Oracle
@@ -746,6 +848,32 @@ def run_reference(args, world, rank) -> dict | None:
                     "oracle, a line-by-line C++ restatement of the reference's CPU path, on all host threads"}
 
 
+def run_reference_pathtrace(args, world) -> dict:
+    scene_path, desc = WORKLOADS[args.workload]
+    with open(os.path.join(ROOT, scene_path)) as f:
+        src = f.read()
+    W = H = PT_FILM
+    vals = []
+    for i in range(args.warmup + args.steps):
+        b = pathtrace_cpu(src, W, H, PT_SPP)
+        if i >= args.warmup:
+            vals.append(b)
+    value = statistics.mean(v["value"] for v in vals)
+    rows = min(PT_CPU_ROWS, H)
+    return {"impl": "reference", "metric": PT_METRIC, "value": value, "unit": "samples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": W * H * PT_SPP / value * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "scene": scene_path, "description": desc, "film": [W, H],
+                       "spp": PT_SPP},
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": vals[0]["cores"], "kind": "port",
+                             "sample": f"each step shades rows 0..{rows} of the film; ms_per_step is the "
+                                       "whole film at that rate", "cpu": vals[0]["cpu"]},
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the Rust reference cannot be built in this image (no rustc/cargo); this arm times the "
+                    "oracle's restatement of reference.rs on all host threads"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -770,6 +898,8 @@ def main():
             line = run_solve_hbm(args, world, rank, local)
         elif args.workload == "c4_multi":
             line = run_multi(args, world, rank, local)
+        elif args.workload == "pathtrace":
+            line = run_pathtrace(args, world, rank, local)
         else:
             line = run_ours(args, world, rank, local)
         if line is not None:

@@ -119,7 +119,8 @@ typedef struct ifx_stats {
 #define IFX_KERNEL_REFLECT 5
 #define IFX_KERNEL_SHADOW2 6
 #define IFX_KERNEL_SHADE_OTHER 7
-#define IFX_NUM_KERNELS 8
+#define IFX_KERNEL_PATH 8 /* the path tracer of ifx_render_reference */
+#define IFX_NUM_KERNELS 9
 #define IFX_WORK_COUNTERS 21
 
 /* ------------------------------------------------------------- scene --- */

@@ -53,7 +53,7 @@ EXPORTS = (
 )
 NOALLOC_MAX_CLUSTERS = 16384
 KERNELS = {"visibility": 0, "closure": 1, "light": 2, "primary": 3, "shadow": 4, "reflect": 5, "shadow2": 6,
-           "shade_other": 7}
+           "shade_other": 7, "path": 8}
 WORK_COUNTERS = 21
 
 

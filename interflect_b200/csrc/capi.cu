@@ -125,7 +125,7 @@ struct ifx_ctx {
     DBuf cub_tmp, small;  // small: 8 x u64 counters / results
     DBuf gen_cand, gen_keep, gen_off, gen_head, gen_pts, gen_next, gen_state, gen_out;  // surfel generation
 
-    // measurement: per-kernel events, work counters (4 kernels x 21 u64), timer
+    // measurement: per-kernel events, work counters (IFX_NUM_KERNELS x 21 u64), timer
     cudaEvent_t kv0 = nullptr, kv1 = nullptr, kc0 = nullptr, kc1 = nullptr, tm0 = nullptr, tm1 = nullptr;
     cudaEvent_t shev[kShadeEvents] = {};
     bool counting = false;
@@ -1455,6 +1455,7 @@ extern "C" int ifx_render_reference(ifx_ctx* ctx, const ifx_camera* cam, uint32_
     ENSURE(ctx->out8, px * 3);
     P.film = (float*)ctx->film.p;
     P.out8 = (uint8_t*)ctx->out8.p;
+    P.counts = ctx->work_of(IFX_KERNEL_PATH);
     unsigned long long* cursor = (unsigned long long*)ctx->qcur.p;
     CK(cudaMemsetAsync(cursor, 0, 8, ctx->st));
     CK(cudaEventRecord(ctx->ev0, ctx->st));

@@ -36,10 +36,11 @@ __device__ __forceinline__ V cosine_hemisphere(V n, Pcg32& rng, const float2* si
     return nrm(t * (r * sc.y) + b * (r * sc.x) + n * sqrtf(fmaxf(1.0f - u1, 0.0f)));
 }
 
-// reference.rs:61-137
+// reference.rs:61-137. `cnt` tallies the tracing work (counting launches
+// only; the timed kernel uses NoCount).
+template <class C>
 __device__ V path(const SceneView& sv, V ro, V rd, float tmax, uint32_t max_depth, Pcg32& rng,
-                  const float2* sincos) {
-    NoCount cnt;
+                  const float2* sincos, C& cnt) {
     V radiance{0.0f, 0.0f, 0.0f}, throughput{1.0f, 1.0f, 1.0f};
     V origin = ro, dir = rd;
     for (uint32_t depth = 0; depth < max_depth; ++depth) {
@@ -87,8 +88,10 @@ __device__ V path(const SceneView& sv, V ro, V rd, float tmax, uint32_t max_dept
     return radiance;
 }
 
+template <class C>
 __global__ void __launch_bounds__(128) k_path(ShadeParams P, uint32_t spp, const float2* sincos,
                                                unsigned long long* cursor) {
+    C cnt;
     IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
     __shared__ float t8[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) t8[i] = P.srgb_t[i];
@@ -102,21 +105,26 @@ __global__ void __launch_bounds__(128) k_path(ShadeParams P, uint32_t spp, const
         const V rd = camera_ray(P, (uint32_t)pix);
         Pcg32 rng(((unsigned long long)y << 32) | (unsigned long long)x);
         V acc{0.0f, 0.0f, 0.0f};
-        for (uint32_t i = 0; i < spp; ++i) acc = acc + path(sv, org, rd, P.tmax, 12u, rng, sincos);
+        for (uint32_t i = 0; i < spp; ++i) acc = acc + path(sv, org, rd, P.tmax, 12u, rng, sincos, cnt);
         write_pixel(P, t8, (uint32_t)pix, acc / (float)spp);
     }
+    if constexpr (sizeof(C) > 1) cnt.flush(P.counts);
 }
 
 int launch_path(cudaStream_t st, const ShadeParams& p, uint32_t spp, const float2* sincos,
                 unsigned long long* cursor) {
     const size_t sm = blob_smem(p.blob, 128);
-    k_path<<<persistent_grid(k_path, 128, sm, (unsigned long long)p.w * p.h), 128, sm, st>>>(p, spp, sincos,
-                                                                                           cursor);
+    const unsigned long long px = (unsigned long long)p.w * p.h;
+    if (p.counts)
+        k_path<Counts><<<persistent_grid(k_path<Counts>, 128, sm, px), 128, sm, st>>>(p, spp, sincos, cursor);
+    else
+        k_path<NoCount><<<persistent_grid(k_path<NoCount>, 128, sm, px), 128, sm, st>>>(p, spp, sincos, cursor);
     return 1;
 }
 
 void configure_path_kernels(int max_dyn_smem) {
-    cudaFuncSetAttribute(k_path, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_path<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_path<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }
 
 }  // namespace ifx

@@ -102,3 +102,27 @@ def test_energy_against_path_traced_ground_truth(tmp_path):
         ratios[name] = float(line.split("ratio")[1].strip(" )"))
     print(ratios)
     assert all(0.85 < v < 1.25 for v in ratios.values()), ratios
+
+
+def test_accuracy_benchmark_runs(tmp_path):
+    """bench.sh's table through `python -m interflect_b200.accuracy`, small."""
+    from interflect_b200 import accuracy
+    r = accuracy.run(spp=16, res=64, out_dir=str(tmp_path))
+    assert r["deterministic"]
+    assert [x["scene"] for x in r["scenes"]] == ["box_only", "cornell", "high_albedo", "sphere_only"]
+    assert all(0.8 < x["luma"] < 1.3 and 0.0 < x["ssim"] <= 1.0 for x in r["scenes"]), r["scenes"]
+    assert set(r["perf_ms"]) == {"cornell", "product", "stress"}
+
+
+def test_path_work_counters(ctx):
+    """The counting launch of the path tracer tallies its marches and SDF
+    queries without changing the image."""
+    ctx.upload(ifx.parse(scene_src("cornell")))
+    plain, _ = ctx.render_reference(16, 16, 2, srgb=False)
+    ctx.set_work_counting(True)
+    ctx.reset_work()
+    counted, _ = ctx.render_reference(16, 16, 2, srgb=False)
+    counts, flops = ctx.work("path")
+    ctx.set_work_counting(False)
+    assert counted.tobytes() == plain.tobytes()
+    assert counts[12] > 0 and counts[11] >= counts[12] and flops > 0
