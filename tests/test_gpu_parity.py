@@ -89,6 +89,13 @@ def test_transfer_parity(ctx, name, target, res):
     assert gi.evals == oi["evals"]
     assert gi.interior_rows == oi["interior_rows"]
     gt, ot = ctx.transfer(), o.transfer(k, oi["links"])
+    # Threshold-boundary mismatches: rows whose set of linked clusters differs
+    # (a visibility or form-factor cut decided the other way). Counted and
+    # reported; the bar is zero.
+    gs_, os_ = gt["starts"].astype(np.int64), ot["starts"].astype(np.int64)
+    mism = sum(1 for i in range(k) if not np.array_equal(gt["idx"][gs_[i]:gs_[i + 1]], ot["idx"][os_[i]:os_[i + 1]]))
+    print(f"{name} res {res}: {k} rows, {gi.links} links, threshold-boundary row mismatches {mism}")
+    assert mism == 0
     assert np.array_equal(gt["starts"], ot["starts"])
     assert np.array_equal(gt["idx"], ot["idx"])
     assert_close(gt["w"], ot["w"], f"{name} link weights")
@@ -123,6 +130,52 @@ def test_light_and_solve_parity(ctx, name, target):
     g, rr = ctx.surfels(), o.surfels()
     assert_close(g["rad"], rr["rad"], f"{name} radiosity")
     assert_close(g["irr"], rr["irr"], f"{name} irradiance")
+
+
+def fp64_solve(direct, albedo, area, carea, offsets, members, starts, idx, w, iterations):
+    """solve.rs:47-108 in FP64 for a fixed bounce count: cluster radiosity as
+    the area-weighted mean of its members, then B = E + rho * sum w B_cluster."""
+    E, rho = direct.astype(np.float64), albedo.astype(np.float64)
+    a = area.astype(np.float64).reshape(-1, 1)
+    offsets, members = offsets.astype(np.int64), members.astype(np.int64)
+    nc = len(offsets) - 1
+    seg = np.repeat(np.arange(nc), np.diff(offsets))
+    carea = carea.astype(np.float64)
+    starts = starts.astype(np.int64)
+    row = np.repeat(np.arange(len(E)), np.diff(starts))
+    wv = w.astype(np.float64).reshape(-1, 1)
+    rad = E.copy()
+    irr = np.zeros_like(E)
+    for _ in range(iterations):
+        crad = np.zeros((nc, 3))
+        np.add.at(crad, seg, rad[members] * a[members])
+        crad /= np.maximum(carea, 1e-12).reshape(-1, 1)
+        irr = np.zeros_like(E)
+        np.add.at(irr, row, crad[idx.astype(np.int64)] * wv)
+        rad = E + rho * irr
+    return rad, irr
+
+
+@pytest.mark.parametrize("name,target", [("product", None), ("cornell", 6000), ("stress", 4000)])
+def test_solve_against_fp64(ctx, name, target):
+    """The GPU's FP32 radiosity against an FP64 solve of the same system (the
+    GPU's own matrix, clusters and E, the same bounce count): max and RMS
+    relative error stated, bounded by 1e-4."""
+    src, o, k, s = pipeline(name, target)
+    r = o.surfels()
+    ctx.upload(s)
+    ctx.upload_surfels(r["p"], r["n"], r["albedo"], r["area"])
+    info = ctx.build(8)
+    ctx.light_surfels()
+    st = ctx.solve(o.info()["bounces"])
+    g, t, c = ctx.surfels(), ctx.transfer(), ctx.clusters(info.clusters)
+    rad64, irr64 = fp64_solve(g["direct"], g["albedo"], g["area"], c["area"], c["offsets"], c["members"], t["starts"],
+                              t["idx"], t["w"], st.iterations)
+    for what, gpu, ref in (("radiosity", g["rad"], rad64), ("irradiance", g["irr"], irr64)):
+        e = rel_err(gpu, ref)
+        print(f"{name} {what} vs FP64 after {st.iterations} bounces: max rel {e.max():.3e}, "
+              f"rms {np.sqrt(np.mean(e ** 2)):.3e}")
+        assert e.max() <= REL
 
 
 def test_solve_alone_bit_exact_from_same_E(ctx):
