@@ -380,10 +380,15 @@ __device__ __forceinline__ float scene_dist(const SceneView& sv, V p, C& cnt) {
 // take part in the votes). Each active lane runs its own near-first BVH
 // traversal with the reference's pruning, but leaves are evaluated in
 // warp-synchronous rounds: a lane advances through interior nodes until it
-// reaches a leaf that passes the AABB test, the warp picks one pending leaf,
-// and every lane waiting on that leaf evaluates its objects together, so the
-// primitive code runs converged. A lane's sequence of node tests, object
-// evaluations and best-distance updates is exactly the one dist_mat() makes.
+// reaches a leaf that passes the AABB test; then, once every lane has either
+// found one or finished, either the lanes sharing the first waiting lane's
+// leaf evaluate it together (the primitive code runs converged) or, in trees
+// of more than four leaves when fewer than half of the waiting lanes share
+// that leaf, every waiting lane evaluates its own leaf in the same round
+// (lanes at different leaves then diverge only by primitive kind, instead of
+// waiting a round per leaf). A lane's sequence of node
+// tests, object evaluations and best-distance updates is exactly the one
+// dist_mat() makes.
 template <class C>
 __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool active, C& cnt) {
     DistHit best{kMaxF, 0u};
@@ -456,8 +461,14 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         const unsigned waiting = __ballot_sync(0xffffffffu, pending >= 0);
         if (!waiting) break;
         const int leaf = __shfl_sync(0xffffffffu, pending, __ffs(waiting) - 1);
-        if (pending == leaf) {
-            const DNode nd = sv.nodes[leaf];
+        // Trees of at most four leaves: one leaf per round, converged. Larger
+        // trees: the first waiting lane's leaf is evaluated alone when at
+        // least half the waiting lanes share it; otherwise every waiting lane
+        // evaluates its own leaf in this round.
+        const bool shared = sv.n_nodes <= 7 || 2 * __popc(__ballot_sync(0xffffffffu, pending == leaf)) >=
+                                                   __popc(waiting);
+        if (pending >= 0 && (pending == leaf || !shared)) {
+            const DNode nd = sv.nodes[pending];
             for (int k = nd.link; k < nd.link + nd.count; ++k) {
                 const DObject o = sv.objs[k];
                 float d = obj_dist(sv, o, p, cnt);
