@@ -298,6 +298,24 @@ int ifx_grid_build(ifx_ctx* ctx, float radius);
 int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
                      float* out_linear, uint8_t* out_srgb, uint64_t* evals);
 
+/* One whole frame on the current surfels (src/main.rs:433-534 after surfel
+ * generation): for the beauty and indirect modes ifx_transfer_build
+ * (cluster_res), ifx_light_surfels, ifx_solve(max_bounces) and
+ * ifx_grid_build(0), then ifx_render_frame(cam, mode, ...), with results
+ * identical to those calls made in that order. The shading passes that read
+ * no GI data (primary hits, their shadow rays, mirror rays and theirs) run
+ * on a second CUDA stream while the GI stages run; only the composition
+ * waits for the grid. Other modes skip the GI stages, as main.rs does. */
+typedef struct ifx_frame_info {
+    ifx_transfer_info transfer; /* as ifx_transfer_build reports it */
+    uint64_t light_evals;       /* ifx_light_surfels */
+    ifx_solve_stats solve;      /* ifx_solve */
+    uint64_t shade_evals;       /* ifx_render_frame's `evals` */
+    float ms_frame;             /* device time of the whole call */
+} ifx_frame_info;
+int ifx_frame(ifx_ctx* ctx, int cluster_res, uint32_t max_bounces, const ifx_camera* cam, int mode, uint32_t w,
+              uint32_t h, float exposure, float* out_linear, uint8_t* out_srgb, ifx_frame_info* out);
+
 /* --------------------------------------------------- differentiation --- */
 /* Gradients of an image loss with respect to per-surfel albedo and per-light
  * emission, geometry and visibility held fixed. None of this has a

@@ -49,7 +49,7 @@ EXPORTS = (
     "ifx_diff_forward", "ifx_diff_backward",
     "ifx_multiscene_create", "ifx_multiscene_destroy", "ifx_multiscene_last_error", "ifx_multiscene_add",
     "ifx_multiscene_build", "ifx_multiscene_run", "ifx_multiscene_download", "ifx_set_stage_limit",
-    "ifx_clusters_build", "ifx_render_reference",
+    "ifx_clusters_build", "ifx_render_reference", "ifx_frame",
 )
 NOALLOC_MAX_CLUSTERS = 16384
 KERNELS = {"visibility": 0, "closure": 1, "light": 2, "primary": 3, "shadow": 4, "reflect": 5, "shadow2": 6,
@@ -92,6 +92,11 @@ class _TransferInfo(C.Structure):
 
 class _SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("residual", C.c_float)]
+
+
+class _FrameInfo(C.Structure):
+    _fields_ = [("transfer", _TransferInfo), ("light_evals", C.c_uint64), ("solve", _SolveStats),
+                ("shade_evals", C.c_uint64), ("ms_frame", C.c_float)]
 
 
 class _Stats(C.Structure):
@@ -171,6 +176,7 @@ def lib() -> C.CDLL:
         "ifx_set_stage_limit": (I, [P, U32]),
         "ifx_clusters_build": (I, [P, I, C.POINTER(U64)]),
         "ifx_render_reference": (I, [P, C.POINTER(_Camera), U32, U32, U32, F, P, P]),
+        "ifx_frame": (I, [P, I, U32, C.POINTER(_Camera), I, U32, U32, F, P, P, C.POINTER(_FrameInfo)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -472,6 +478,32 @@ class Context:
         self._check(lib().ifx_render_frame(self._h, C.byref(cam) if cam is not None else None, m, width, height,
                                            exposure, _ptr(lin), _ptr(s8), C.byref(e)), "render_frame")
         return lin, s8, e.value
+
+    def frame(self, width: int, height: int, mode="beauty", cluster_res: int = 8, max_bounces: int | None = None,
+              cam=None, exposure: float | None = None, linear: bool = True, srgb: bool = True) -> dict:
+        """The transfer build, light_surfels, solve, grid and render_frame in
+        one call, the GI-independent shading passes overlapped with the GI
+        stages. Returns dict(linear, srgb, transfer, light_evals, solve,
+        shade_evals, ms_frame)."""
+        m = MODES[mode] if isinstance(mode, str) else int(mode)
+        cfg = self.scene.cfg if self.scene is not None else None
+        if exposure is None:
+            exposure = cfg.exposure if cfg is not None else 1.0
+        if max_bounces is None:
+            max_bounces = cfg.bounces if cfg is not None else 16
+        lin = np.zeros((height, width, 3), np.float32) if linear else None
+        s8 = np.zeros((height, width, 3), np.uint8) if srgb else None
+        fi = _FrameInfo()
+        self._check(lib().ifx_frame(self._h, cluster_res, max_bounces, C.byref(cam) if cam is not None else None, m,
+                                    width, height, exposure, _ptr(lin), _ptr(s8), C.byref(fi)), "frame")
+        t = fi.transfer
+        if m in (MODES["beauty"], MODES["indirect"]):
+            self._tinfo = TransferInfo(t.clusters, t.links, t.candidates, t.evals, t.interior_rows, t.mean_row_sum)
+        return dict(linear=lin, srgb=s8,
+                    transfer=TransferInfo(t.clusters, t.links, t.candidates, t.evals, t.interior_rows,
+                                          t.mean_row_sum),
+                    light_evals=fi.light_evals, solve=SolveStats(fi.solve.iterations, fi.solve.residual),
+                    shade_evals=fi.shade_evals, ms_frame=fi.ms_frame)
 
     def render_reference(self, width: int, height: int, spp: int = 512, cam=None, exposure: float | None = None,
                          linear: bool = True, srgb: bool = True):

@@ -98,6 +98,12 @@ struct ifx_ctx {
     // film
     DBuf film, out8;
     DBuf path_sincos;  // (sinf, cosf) of the path tracer's 2^24 sampler angles
+    // ifx_frame: the second stream that runs the shading passes beside the
+    // GI stages, its scratch (16 cursors, the SDF evaluation counter) and
+    // events (fork, join, start and end of its work).
+    cudaStream_t st2 = nullptr;
+    DBuf shsc;
+    cudaEvent_t fev[4] = {};
 
     // lights: current emission per light (float4), for the relight and adjoint
     DBuf lemit;
@@ -349,6 +355,10 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
         if ((e = cudaEventCreate(ev)) != cudaSuccess) return bail(e);
     for (int i = 0; i < kShadeEvents; ++i)
         if ((e = cudaEventCreate(&ctx->shev[i])) != cudaSuccess) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    for (cudaEvent_t& ev : ctx->fev)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
+    if (ensure(ctx, ctx->shsc, 32 * 8) != IFX_OK) return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->work, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8) != IFX_OK ||
         cudaMemsetAsync(ctx->work.p, 0, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8, ctx->st) != cudaSuccess)
         return bail(cudaErrorMemoryAllocation);
@@ -381,6 +391,7 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     for (ifx_multiscene* ms : ctx->owners) multiscene_forget(ms, ctx);
     cudaSetDevice(ctx->device);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
+    if (ctx->st2) cudaStreamSynchronize(ctx->st2);
     DBuf* bufs[] = {&ctx->blob, &ctx->status, &ctx->srgb_t, &ctx->sp, &ctx->sn, &ctx->salb, &ctx->sdir, &ctx->sirr,
                     &ctx->srad, &ctx->keys, &ctx->keys_alt, &ctx->heads, &ctx->head_scan, &ctx->seg_start,
                     &ctx->members, &ctx->cp_tmp, &ctx->cn_tmp, &ctx->valid, &ctx->valid_scan, &ctx->cp, &ctx->cn,
@@ -399,13 +410,16 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->ft, &ctx->ftstarts, &ctx->cid, &ctx->hist, &ctx->dg, &ctx->h_t, &ctx->yv, &ctx->ebar,
                     &ctx->rhobar, &ctx->epart, &ctx->eout, &ctx->d3, &ctx->sell_len, &ctx->sell_perm, &ctx->sell_keys,
                     &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w,
-                    &ctx->path_sincos};
+                    &ctx->path_sincos, &ctx->shsc};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : ctx->shev)
         if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ctx->fev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->st2) cudaStreamDestroy(ctx->st2);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }
@@ -1297,13 +1311,10 @@ extern "C" int ifx_grid_build(ifx_ctx* ctx, float radius) {
 
 // keep_film: the linear film stays in device memory (ctx->film) even when no
 // host copy is asked for; saved (nullable) receives the launch parameters.
-static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
-                       float* out_linear, uint8_t* out_srgb, uint64_t* evals, bool keep_film, ShadeParams* saved) {
-    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
-    if (mode < 0 || mode > 5) return fail(ctx, IFX_ERR_INVALID, "unknown mode");
-    if (w == 0 || h == 0 || w > 16384u || h > 16384u || (uint64_t)w * h > 40000000ull)
-        return fail(ctx, IFX_ERR_LIMIT, "film size out of range");
-    CK(cudaSetDevice(ctx->device));
+// The parameters and wavefront buffers of one render_frame pass (no
+// launches). `has_gi`: the passes that need the gather grid run.
+static int shade_prepare(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
+                         bool keep_film, bool has_gi, ShadeParams& P) {
     const HScene& s = ctx->scene;
     F3 pos = s.camera.pos, look = s.camera.look, up = s.camera.up;
     float fov = s.camera.fov;
@@ -1314,10 +1325,9 @@ static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w
         fov = cam->fov;
     }
     CamBasis b = camera_basis(pos, look, up, fov, w, h);
-    ShadeParams P{};
+    P = ShadeParams{};
     P.blob = ctx->blobref;
-    const bool needs_gi = mode == IFX_MODE_BEAUTY || mode == IFX_MODE_INDIRECT;
-    P.has_gi = needs_gi && ctx->has_grid ? 1 : 0;
+    P.has_gi = has_gi ? 1 : 0;
     P.grid = ctx->grid;
     memcpy(P.cam.origin, b.origin, 12);
     memcpy(P.cam.fwd, b.fwd, 12);
@@ -1333,7 +1343,7 @@ static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w
     P.tonemap = mode <= IFX_MODE_INDIRECT ? 1 : 0;
     P.srgb_t = (const float*)ctx->srgb_t.p;
     size_t px = (size_t)w * h;
-    if (out_linear || keep_film) {
+    if (keep_film) {
         ENSURE(ctx->film, px * 12);
         P.film = (float*)ctx->film.p;
     }
@@ -1373,6 +1383,22 @@ static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w
     P.qlen = (uint32_t*)ctx->qlen.p;
     P.cursors = (unsigned long long*)ctx->qcur.p;
     P.nl = nl;
+    return IFX_OK;
+}
+
+static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, uint32_t h, float exposure,
+                       float* out_linear, uint8_t* out_srgb, uint64_t* evals, bool keep_film, ShadeParams* saved) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (mode < 0 || mode > 5) return fail(ctx, IFX_ERR_INVALID, "unknown mode");
+    if (w == 0 || h == 0 || w > 16384u || h > 16384u || (uint64_t)w * h > 40000000ull)
+        return fail(ctx, IFX_ERR_LIMIT, "film size out of range");
+    CK(cudaSetDevice(ctx->device));
+    const bool needs_gi = mode == IFX_MODE_BEAUTY || mode == IFX_MODE_INDIRECT;
+    ShadeParams P;
+    int r = shade_prepare(ctx, cam, mode, w, h, exposure, out_linear || keep_film, needs_gi && ctx->has_grid, P);
+    if (r) return r;
+    const size_t px = (size_t)w * h;
+    unsigned long long* small = (unsigned long long*)ctx->small.p;
     CK(cudaMemsetAsync(&small[3], 0, 8, ctx->st));
     CK(cudaMemsetAsync(ctx->qlen.p, 0, 16, ctx->st));
     CK(cudaMemsetAsync(ctx->qcur.p, 0, 16 * 8, ctx->st));
@@ -1384,7 +1410,7 @@ static int render_impl(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w
     CK(cudaMemcpyAsync(&e, &small[3], 8, cudaMemcpyDeviceToHost, ctx->st));
     if (out_linear) CK(cudaMemcpyAsync(out_linear, ctx->film.p, px * 12, cudaMemcpyDeviceToHost, ctx->st));
     if (out_srgb) CK(cudaMemcpyAsync(out_srgb, ctx->out8.p, px * 3, cudaMemcpyDeviceToHost, ctx->st));
-    int r = check_status(ctx);
+    r = check_status(ctx);
     if (r) return r;
     CK(cudaEventElapsedTime(&ctx->stats.ms_shade, ctx->ev0, ctx->ev1));
     float g[7];
@@ -1474,6 +1500,87 @@ extern "C" int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, u
                                 float* out_linear, uint8_t* out_srgb, uint64_t* evals) {
     if (ctx) frame_changed(ctx);  // the wavefront buffers are about to be overwritten
     return render_impl(ctx, cam, mode, w, h, exposure, out_linear, out_srgb, evals, false, nullptr);
+}
+
+// main.rs:433-534 in one call. The GI stages run on ctx->st exactly as the
+// stage calls run them (their host synchronisations wait for that stream
+// only); the shading passes that read no GI data run meanwhile on ctx->st2
+// with their own cursors, counter and status word, and the composition
+// waits for the grid. Every buffer either side writes belongs to that side.
+extern "C" int ifx_frame(ifx_ctx* ctx, int cluster_res, uint32_t max_bounces, const ifx_camera* cam, int mode,
+                         uint32_t w, uint32_t h, float exposure, float* out_linear, uint8_t* out_srgb,
+                         ifx_frame_info* out) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    if (mode < 0 || mode > 5) return fail(ctx, IFX_ERR_INVALID, "unknown mode");
+    if (w == 0 || h == 0 || w > 16384u || h > 16384u || (uint64_t)w * h > 40000000ull)
+        return fail(ctx, IFX_ERR_LIMIT, "film size out of range");
+    if (cluster_res < 1 || cluster_res > 512) return fail(ctx, IFX_ERR_LIMIT, "cluster resolution must be in 1..512");
+    CK(cudaSetDevice(ctx->device));
+    frame_changed(ctx);
+    const bool needs_gi = mode == IFX_MODE_BEAUTY || mode == IFX_MODE_INDIRECT;  // main.rs:42-44
+    if (needs_gi && ctx->n == 0) return fail(ctx, IFX_ERR_INVALID, "no surfels");
+    ifx_frame_info info{};
+    ShadeParams P;
+    int r = shade_prepare(ctx, cam, mode, w, h, exposure, out_linear != nullptr, needs_gi, P);
+    if (r) return r;
+    unsigned long long* sc = (unsigned long long*)ctx->shsc.p;
+    P.cursors = sc;
+    P.evals = &sc[16];
+    P.status = (uint32_t*)ctx->status.p + 1;
+    cudaStream_t st2 = ctx->st2;
+    // Fork: the second stream starts after everything queued so far.
+    CK(cudaEventRecord(ctx->fev[0], ctx->st));
+    CK(cudaStreamWaitEvent(st2, ctx->fev[0], 0));
+    CK(cudaMemsetAsync(sc, 0, 17 * 8, st2));
+    CK(cudaMemsetAsync(ctx->qlen.p, 0, 16, st2));
+    CK(cudaEventRecord(ctx->fev[2], st2));
+    ctx->launches += (uint64_t)launch_shade(st2, P, ctx->shev, kShadeFront);
+    // Whatever happens on ctx->st from here, the second stream is drained
+    // before this call returns.
+    auto finish = [&](int code) {
+        cudaStreamSynchronize(st2);
+        return code;
+    };
+    if (cudaGetLastError() != cudaSuccess) return finish(fail(ctx, IFX_ERR_CUDA, "launch failed"));
+    if (needs_gi) {
+        if ((r = ifx_transfer_build(ctx, cluster_res, &info.transfer))) return finish(r);
+        if ((r = ifx_light_surfels(ctx, &info.light_evals))) return finish(r);
+        if ((r = ifx_solve(ctx, max_bounces, &info.solve))) return finish(r);
+        if ((r = ifx_grid_build(ctx, 0.0f))) return finish(r);
+        P.grid = ctx->grid;
+    }
+    // Join: the composition waits for the grid, then ctx->st waits for it.
+    CK(cudaEventRecord(ctx->fev[1], ctx->st));
+    CK(cudaStreamWaitEvent(st2, ctx->fev[1], 0));
+    ctx->launches += (uint64_t)launch_shade(st2, P, ctx->shev, kShadeCompose);
+    if (cudaGetLastError() != cudaSuccess) return finish(fail(ctx, IFX_ERR_CUDA, "launch failed"));
+    CK(cudaEventRecord(ctx->fev[3], st2));
+    const size_t px = (size_t)w * h;
+    unsigned long long e = 0;
+    uint32_t status = 0;
+    CK(cudaMemcpyAsync(&e, &sc[16], 8, cudaMemcpyDeviceToHost, st2));
+    CK(cudaMemcpyAsync(&status, P.status, 4, cudaMemcpyDeviceToHost, st2));
+    if (out_linear) CK(cudaMemcpyAsync(out_linear, ctx->film.p, px * 12, cudaMemcpyDeviceToHost, st2));
+    if (out_srgb) CK(cudaMemcpyAsync(out_srgb, ctx->out8.p, px * 3, cudaMemcpyDeviceToHost, st2));
+    CK(cudaStreamWaitEvent(ctx->st, ctx->fev[3], 0));
+    CK(cudaStreamSynchronize(st2));
+    if (status) {
+        CK(cudaMemsetAsync(P.status, 0, 4, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        return fail(ctx, IFX_ERR_TIMEOUT, "a device-side bounded wait expired (status 0x" + std::to_string(status) + ")");
+    }
+    CK(cudaEventElapsedTime(&ctx->stats.ms_shade, ctx->fev[2], ctx->fev[3]));
+    float g[7];
+    for (int i = 0; i < 7; ++i) CK(cudaEventElapsedTime(&g[i], ctx->shev[2 * i], ctx->shev[2 * i + 1]));
+    ctx->stats.ms_primary = g[0];
+    ctx->stats.ms_shadow = g[1];
+    ctx->stats.ms_reflect = g[2];
+    ctx->stats.ms_shadow2 = g[3];
+    ctx->stats.ms_shade_other = g[4] + g[5] + g[6];
+    CK(cudaEventElapsedTime(&info.ms_frame, ctx->fev[0], ctx->fev[3]));
+    info.shade_evals = e;
+    if (out) *out = info;
+    return IFX_OK;
 }
 
 // ------------------------------------------------------ differentiation ---

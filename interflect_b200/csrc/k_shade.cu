@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(128) k_compose(ShadeParams P) {
 // slots (kNumCounters u64 each) 0 primary, 1 shadow, 2 reflect, 3 shadow2,
 // 4 the rest.
 template <class C>
-static void launch_all(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev) {
+static void launch_all(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev, int part) {
     const size_t sm = blob_smem(p.blob, 128);
     const unsigned long long px = (unsigned long long)p.w * p.h;
     const unsigned long long slots = px * (unsigned long long)(p.nl > 0 ? p.nl : 1);
@@ -288,37 +288,40 @@ static void launch_all(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev) {
     auto rec = [&](int i) {
         if (ev) cudaEventRecord(ev[i], st);
     };
-    rec(0);
-    k_primary<C><<<persistent_grid(k_primary<C>, 128, sm, px), 128, sm, st>>>(with(0));
-    rec(1);
-    rec(8);
-    k_setup<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
-    rec(9);
-    rec(2);
-    k_shadow<C><<<persistent_grid(k_shadow<C>, 128, sm, slots), 128, sm, st>>>(with(1), p.hp1, p.hn1, p.q1,
-                                                                                &p.qlen[0], p.vis1, &p.cursors[2]);
-    rec(3);
-    rec(4);
-    if (p.has_gi) k_reflect<C><<<persistent_grid(k_reflect<C>, 128, sm, px), 128, sm, st>>>(with(2));
-    rec(5);
-    rec(10);
-    if (p.has_gi) k_setup2<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
-    rec(11);
-    rec(6);
-    if (p.has_gi)
-        k_shadow<C><<<persistent_grid(k_shadow<C>, 128, sm, slots), 128, sm, st>>>(with(3), p.hp2, p.hn2, p.q2,
-                                                                                    &p.qlen[2], p.vis2,
-                                                                                    &p.cursors[3]);
-    rec(7);
-    rec(12);
-    k_compose<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
-    rec(13);
+    if (part & kShadeFront) {
+        rec(0);
+        k_primary<C><<<persistent_grid(k_primary<C>, 128, sm, px), 128, sm, st>>>(with(0));
+        rec(1);
+        rec(8);
+        k_setup<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
+        rec(9);
+        rec(2);
+        k_shadow<C><<<persistent_grid(k_shadow<C>, 128, sm, slots), 128, sm, st>>>(
+            with(1), p.hp1, p.hn1, p.q1, &p.qlen[0], p.vis1, &p.cursors[2]);
+        rec(3);
+        rec(4);
+        if (p.has_gi) k_reflect<C><<<persistent_grid(k_reflect<C>, 128, sm, px), 128, sm, st>>>(with(2));
+        rec(5);
+        rec(10);
+        if (p.has_gi) k_setup2<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
+        rec(11);
+        rec(6);
+        if (p.has_gi)
+            k_shadow<C><<<persistent_grid(k_shadow<C>, 128, sm, slots), 128, sm, st>>>(
+                with(3), p.hp2, p.hn2, p.q2, &p.qlen[2], p.vis2, &p.cursors[3]);
+        rec(7);
+    }
+    if (part & kShadeCompose) {
+        rec(12);
+        k_compose<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
+        rec(13);
+    }
 }
 
-int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev) {
-    if (p.counts) launch_all<Counts>(st, p, ev);
-    else launch_all<NoCount>(st, p, ev);
-    return p.has_gi ? 7 : 4;
+int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev, int part) {
+    if (p.counts) launch_all<Counts>(st, p, ev, part);
+    else launch_all<NoCount>(st, p, ev, part);
+    return ((part & kShadeFront) ? (p.has_gi ? 6 : 3) : 0) + ((part & kShadeCompose) ? 1 : 0);
 }
 
 int launch_compose(cudaStream_t st, const ShadeParams& p) {

@@ -209,8 +209,12 @@ struct ShadeParams {
 // Returns the number of kernels launched. `ev` (nullable) holds
 // kShadeEvents events recorded around the kernels (see k_shade.cu);
 // p.counts (nullable) points at 5 consecutive counter slots.
+// `part` selects the passes before the composition (primary hits, their
+// shadow rays, mirror rays and theirs: nothing there reads the gather grid),
+// the composition, or both.
 static constexpr int kShadeEvents = 14;
-int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev);
+enum : int { kShadeFront = 1, kShadeCompose = 2, kShadeAll = 3 };
+int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev, int part = kShadeAll);
 // k_compose alone over the hits, form factors and visibilities a previous
 // launch_shade with the same parameters left in the wavefront buffers.
 int launch_compose(cudaStream_t st, const ShadeParams& p);

@@ -291,3 +291,37 @@ def test_product_golden_counts_on_gpu(ctx):
     _, _, ev = ctx.render_frame(s.cfg.width, s.cfg.height)
     assert f"{ev / 1e6:.1f}" == g["shade_evals_M_1dp"]
     assert round(ev / (s.cfg.width * s.cfg.height)) == g["evals_per_px"]
+
+
+@pytest.mark.parametrize("name,target,mode,w,h", [("product", 6000, "beauty", 160, 120),
+                                                  ("stress", 4000, "beauty", 100, 75),
+                                                  ("cornell", 6000, "indirect", 96, 96),
+                                                  ("product", 6000, "direct", 96, 72),
+                                                  ("product", 6000, "normals", 64, 48)])
+def test_fused_frame_matches_stage_calls(ctx, name, target, mode, w, h):
+    """ifx_frame (GI stages on one stream, GI-free shading passes on another)
+    gives exactly what the stage calls give in order: bytes of the film, the
+    matrix and the radiosity, and every count."""
+    s = ifx.parse(scene_src(name))
+    ctx.upload(s)
+    n = ctx.generate(target)
+    gi = mode in ("beauty", "indirect")
+    if gi:
+        info = ctx.build(8)
+        le = ctx.light_surfels()
+        st = ctx.solve(s.cfg.bounces)
+        ctx.grid_build()
+        t0, r0 = ctx.transfer(), ctx.surfels()["rad"]
+    lin0, s80, ev0 = ctx.render_frame(w, h, mode)
+    for _ in range(2):  # twice: the second call runs on grown buffers
+        ctx.upload(s)
+        assert ctx.generate(target) == n
+        f = ctx.frame(w, h, mode, cluster_res=8, max_bounces=s.cfg.bounces)
+        assert f["linear"].tobytes() == lin0.tobytes() and f["srgb"].tobytes() == s80.tobytes()
+        assert f["shade_evals"] == ev0
+        if gi:
+            assert f["transfer"] == info and f["light_evals"] == le and f["solve"] == st
+            t1 = ctx.transfer()
+            assert all(t1[k].tobytes() == t0[k].tobytes() for k in ("starts", "idx", "w"))
+            assert ctx.surfels()["rad"].tobytes() == r0.tobytes()
+        assert f["ms_frame"] > 0.0
