@@ -368,6 +368,9 @@ def run_batch(args, world, rank, local) -> dict | None:
         ctx.solve_batched(None, bounces, outputs=False, R=R)
     flusher = L2Flusher(local)
     barrier(world)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
     launches0 = ctx.stats()["kernel_launches"]
     total_ms = 0.0
     for _ in range(args.steps):
@@ -376,6 +379,7 @@ def run_batch(args, world, rank, local) -> dict | None:
         _, _, its, _ = ctx.solve_batched(None, bounces, outputs=False, R=R)
         total_ms += ctx.timer_stop()
     launches = ctx.stats()["kernel_launches"] - launches0
+    clocks = sampler.stop() if sampler else None
     # End to end: right-hand sides from host memory, radiosity back to host.
     e2e_ms = 0.0
     for _ in range(args.steps):
@@ -408,6 +412,7 @@ def run_batch(args, world, rank, local) -> dict | None:
         "e2e": {"value": R * args.steps / (e2e_max / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(E.nbytes), "d2h_bytes_per_step": int(2 * E.nbytes)},
         "gpu_launches": int(launches),
+        "clocks": clocks,
     }
 
 
@@ -436,10 +441,14 @@ def run_multi(args, world, rank, local) -> dict | None:
     for _ in range(args.warmup):
         ms.run()
     barrier(world)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
     packed = []
     for _ in range(args.steps):
         flusher.flush()
         packed.append(ms.run())
+    clocks = sampler.stop() if sampler else None
     iters = [ms.download(i, linear=False, srgb=False)[2].iterations for i in range(len(members))]
     # (a) One packed launch per scene (the unbatched form of the same work).
     singles = []
@@ -507,6 +516,7 @@ def run_multi(args, world, rank, local) -> dict | None:
         "e2e": {"value": S / (e_max / 1e3), "unit": "scenes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
                 "includes": "graph replay and every scene's sRGB frame downloaded to host"},
         "gpu_launches": args.steps,
+        "clocks": clocks,
     }
 
 
@@ -551,10 +561,14 @@ def run_solve_hbm(args, world, rank, local) -> dict | None:
 
     for _ in range(args.warmup):
         once()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
     times, st = [], None
     for _ in range(args.steps):
         st, ms = once()
         times.append(ms)
+    clocks = sampler.stop() if sampler else None
     rad_sell = ctx.surfels()["rad"]
     # The CSR kernel on the same matrix (caller-owned device copies).
     dev = torch.device(f"cuda:{local}")
@@ -608,6 +622,7 @@ def run_solve_hbm(args, world, rank, local) -> dict | None:
         "csr_kernel": {"value": bpb * st.iterations / (csr_max / 1e3) / 1e9, "unit": "GB/s",
                        "ms": csr_max, "bit_identical_to_sliced_ell": same},
         "gpu_launches": 3 * st.iterations * args.steps,
+        "clocks": clocks,
     }
 
 
@@ -649,6 +664,9 @@ def run_diff(args, world, rank, local) -> dict | None:
         img = ctx.diff_forward(rho0, emit0)
         ctx.diff_backward(2.0 * (img - target))
     barrier(world)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
     launches0 = ctx.stats()["kernel_launches"]
     dev_f, dev_b, e2e = [], [], []
     for _ in range(args.steps):
@@ -662,6 +680,7 @@ def run_diff(args, world, rank, local) -> dict | None:
         dev_f.append(st["ms_diff_forward"])
         dev_b.append(st["ms_diff_backward"])
     launches = ctx.stats()["kernel_launches"] - launches0
+    clocks = sampler.stop() if sampler else None
     (grad_max, fwd_max, e2e_max), _ = allreduce_max_sum(
         [statistics.median([f + b for f, b in zip(dev_f, dev_b)]), statistics.median(fwd), statistics.median(e2e)],
         [0.0], world)
@@ -685,6 +704,7 @@ def run_diff(args, world, rank, local) -> dict | None:
                 "d2h_bytes_per_step": int(img.nbytes + g_rho.nbytes + g_e.nbytes),
                 "includes": "albedo+emission upload, frame download, host loss gradient, adjoint, gradient download"},
         "gpu_launches": int(launches),
+        "clocks": clocks,
     }
 
 
