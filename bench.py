@@ -210,6 +210,8 @@ def run_ours(args, world, rank, local) -> dict | None:
     if args.film:
         fw, fh = (int(v) for v in args.film.lower().split("x"))
         scene.set_cfg(width=fw, height=fh)
+    if args.surfels:
+        scene.set_cfg(surfels=args.surfels)
     cfg = scene.cfg
     ctx = ifx.Context(local)
     ctx.upload(scene)
@@ -920,6 +922,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rows", type=float, default=1.0, help="fraction of film rows the CPU legs shade")
     ap.add_argument("--film", default=None, help="WxH film override for small profiling cases (e.g. 640x360)")
+    ap.add_argument("--surfels", type=int, default=None, help="surfel target override for small profiling cases")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup()

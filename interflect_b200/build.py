@@ -30,7 +30,8 @@ COMPARE = os.path.join(HERE, "bin", "compare")
 CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "k_batch.cu", "k_diff.cu", "k_multi.cu",
               "k_path.cu", "capi.cu", "noalloc.cu"]
 CPP_SOURCES = ["scene_host.cpp"]
-HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh", "shade.cuh", "flop_model.h"]
+HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh", "shade.cuh", "flop_model.h",
+           "sqcmp.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "layout.h"
+#include "sqcmp.h"
 
 namespace ifx {
 
@@ -282,12 +283,14 @@ __device__ __forceinline__ float obj_dist(const SceneView& sv, const DObject& o,
     return d;
 }
 
-// bvh.rs:46-50
+// bvh.rs:46-50 before its square root: the box distance is
+// sqrtf(aabb_dist2(p, n)).
 template <class C>
-__device__ __forceinline__ float aabb_dist(V p, const DNode& n, C& cnt) {
+__device__ __forceinline__ float aabb_dist2(V p, const DNode& n, C& cnt) {
     cnt.add(CN_NODE);
     V lo{n.lo[0], n.lo[1], n.lo[2]}, hi{n.hi[0], n.hi[1], n.hi[2]};
-    return len(vmax(vmax(lo - p, p - hi), V{0.0f, 0.0f, 0.0f}));
+    const V q = vmax(vmax(lo - p, p - hi), V{0.0f, 0.0f, 0.0f});
+    return dot(q, q);
 }
 
 struct DistHit {
@@ -311,12 +314,13 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
         // the node, so the value computed when it was pushed (bvh.rs:135-136)
         // is the one the reference recomputes when it pops it (:116); it is
         // kept on the stack and counted as the reference's test.
+        // The stack holds squared box distances (see sq_ge / sq_lt).
         uint32_t* const stack = sv.stk;
         float* const stackd = sv.stkd;
         const int stride = sv.stk_stride;
         int sp = 0;
         stack[0] = 0;
-        stackd[0] = aabb_dist(p, sv.nodes[0], cnt);
+        stackd[0] = aabb_dist2(p, sv.nodes[0], cnt);
         sp = 1;
         bool first = true;
         while (sp > 0) {
@@ -325,7 +329,7 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
             const DNode nd = sv.nodes[ni];
             if (!first) cnt.add(CN_NODE);
             first = false;
-            if (stackd[sp * stride] >= best.d) continue;
+            if (sq_ge(stackd[sp * stride], best.d)) continue;
             if (nd.count > 0) {
                 for (int k = nd.link; k < nd.link + nd.count; ++k) {
                     const DObject o = sv.objs[k];
@@ -337,14 +341,14 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
                 }
             } else {
                 const int l = ni + 1, r = nd.link;
-                float dl = aabb_dist(p, sv.nodes[l], cnt);
-                float dr = aabb_dist(p, sv.nodes[r], cnt);
+                float dl = aabb_dist2(p, sv.nodes[l], cnt);
+                float dr = aabb_dist2(p, sv.nodes[r], cnt);
                 // Near-first DFS holds at most depth + 1 entries; the host
                 // sizes the stack to depth + 2 (and rejects trees deeper
                 // than the reference's 64-entry stack). The guard keeps an
                 // unexpected overflow inside the stack: traversal stops.
                 if (sp + 2 > sv.stk_depth) break;
-                if (dl < dr) {
+                if (sq_lt(dl, dr)) {
                     stack[sp * stride] = (uint32_t)r;
                     stackd[sp * stride] = dr;
                     stack[(sp + 1) * stride] = (uint32_t)l;
@@ -421,7 +425,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
     bool first = true;
     if (active) {
         stack[0] = 0;
-        stackd[0] = aabb_dist(p, sv.nodes[0], cnt);
+        stackd[0] = aabb_dist2(p, sv.nodes[0], cnt);
         sp = 1;
     }
     int pending = -1;
@@ -433,19 +437,19 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
             // The box distance stored at push time (see dist_mat).
             if (!first) cnt.add(CN_NODE);
             first = false;
-            if (stackd[sp * stride] >= best.d) continue;
+            if (sq_ge(stackd[sp * stride], best.d)) continue;
             if (nd.count > 0) {
                 pending = ni;
                 break;
             }
             const int l = ni + 1, r = nd.link;
-            float dl = aabb_dist(p, sv.nodes[l], cnt);
-            float dr = aabb_dist(p, sv.nodes[r], cnt);
+            float dl = aabb_dist2(p, sv.nodes[l], cnt);
+            float dr = aabb_dist2(p, sv.nodes[r], cnt);
             if (sp + 2 > sv.stk_depth) {
                 sp = 0;
                 break;
             }
-            if (dl < dr) {
+            if (sq_lt(dl, dr)) {
                 stack[sp * stride] = (uint32_t)r;
                 stackd[sp * stride] = dr;
                 stack[(sp + 1) * stride] = (uint32_t)l;
