@@ -305,6 +305,20 @@ def run_ours(args, world, rank, local) -> dict | None:
         with open(tj) as f:
             traffic = json.load(f).get(args.workload, {}).get(dom)
 
+    # Issue-slot roofline of the same kernel: its warp instructions per launch
+    # (ncu, the same workload) over the live duration, against 148 SMs x 4
+    # schedulers x the SM clock sampled during the timed region.
+    issue = None
+    ij = os.path.join(ROOT, "profiles", "ncu_issue.json")
+    if os.path.exists(ij) and not args.film and not args.surfels:
+        with open(ij) as f:
+            inst = json.load(f).get(args.workload, {}).get(dom)
+        mhz = (clocks or {}).get("sm_mhz") or peaks.get("sm_max_mhz") or 1965.0
+        if inst:
+            slots = N_SMS * 4 * mhz * 1e6 * (avg[dom] / 1e3)
+            issue = {"warp_inst_per_launch": inst, "issue_slots_per_launch": slots, "frac": inst / slots,
+                     "sm_mhz": mhz, "source": "profiles/ncu_issue.json (ncu smsp__inst_executed.sum)"}
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -327,7 +341,7 @@ def run_ours(args, world, rank, local) -> dict | None:
         "roofline": {"kernel": dom, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "flops_per_launch": flops, "peak_source": f"fp32 CUDA-core peak from {peak_src}",
-                     "work": {k: float(v[1]) for k, v in work.items()}},
+                     "work": {k: float(v[1]) for k, v in work.items()}, "issue": issue},
         "e2e": {"value": e2e_ev_sum / (e2e_max / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_max / args.steps},
         "gpu_launches": int(launches),

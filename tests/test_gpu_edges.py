@@ -105,3 +105,28 @@ def test_cluster_grid_extremes(ctx, res):
 def test_ragged_films(ctx, w, h):
     o, s = both("product", 3000)
     run_pipeline(ctx, o, s, 3000, 8, 4, w, h)
+
+
+def test_fused_frame_rejects_bad_calls():
+    """ifx_frame validates like the stage calls and leaves the context usable."""
+    c = ifx.Context(0)
+    try:
+        with pytest.raises(ifx.DeviceError):
+            c.frame(16, 16)  # no scene yet
+        s = ifx.parse(scene_src("cornell"))
+        c.upload(s)
+        with pytest.raises(ifx.DeviceError):
+            c.frame(16, 16)  # beauty needs surfels
+        c.generate(2000)
+        with pytest.raises(ifx.LimitError):
+            c.frame(16, 16, cluster_res=0)
+        with pytest.raises(ifx.LimitError):
+            c.frame(0, 16)
+        with pytest.raises(ifx.DeviceError):
+            c.frame(16, 16, mode=7)
+        f = c.frame(16, 16)  # still usable
+        assert f["solve"].iterations > 0 and f["shade_evals"] > 0
+        lin, _, ev = c.render_frame(16, 16)
+        assert lin.tobytes() == f["linear"].tobytes() and ev == f["shade_evals"]
+    finally:
+        c.close()
