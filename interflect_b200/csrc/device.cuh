@@ -380,6 +380,60 @@ __device__ __forceinline__ float scene_dist(const SceneView& sv, V p, C& cnt) {
     return dist_mat(sv, p, cnt).d;
 }
 
+// Evaluates leaf `leaf`'s objects into `best` (bvh.rs:118-126).
+template <class C>
+__device__ __forceinline__ void leaf_eval(const SceneView& sv, int leaf, V p, DistHit& best, C& cnt) {
+    const DNode nd = sv.nodes[leaf];
+    for (int k = nd.link; k < nd.link + nd.count; ++k) {
+        const DObject o = sv.objs[k];
+        const float d = obj_dist(sv, o, p, cnt);
+        if (d < best.d) {
+            best.d = d;
+            best.mat = o.mat;
+        }
+    }
+}
+
+// dist_mat_warp's traversal for a three-node tree (a root and two leaves):
+// the same box tests, pruning decisions, visit order and counts, with the two
+// pending leaves held in registers instead of the shared-memory stack. The
+// root is popped first (not counted, as in dist_mat), then the nearer leaf,
+// then the other; leaves are evaluated in warp rounds of one leaf each.
+template <class C>
+__device__ __forceinline__ DistHit dist_mat_warp3(const SceneView& sv, V p, bool active, DistHit best, C& cnt) {
+    int next = -1, last = -1;  // leaves still to pop, in order
+    float dnext = 0.0f, dlast = 0.0f;
+    if (active) {
+        const float d0 = aabb_dist2(p, sv.nodes[0], cnt);
+        if (!sq_ge(d0, best.d)) {
+            const int l = 1, r = sv.nodes[0].link;
+            const float dl = aabb_dist2(p, sv.nodes[l], cnt);
+            const float dr = aabb_dist2(p, sv.nodes[r], cnt);
+            if (sq_lt(dl, dr)) {
+                next = l, dnext = dl, last = r, dlast = dr;
+            } else {
+                next = r, dnext = dr, last = l, dlast = dl;
+            }
+        }
+    }
+    int pending = -1;
+    while (true) {
+        while (pending < 0 && next >= 0) {
+            cnt.add(CN_NODE);
+            if (!sq_ge(dnext, best.d)) pending = next;
+            next = last, dnext = dlast, last = -1;
+        }
+        const unsigned waiting = __ballot_sync(0xffffffffu, pending >= 0);
+        if (!waiting) break;
+        const int leaf = __shfl_sync(0xffffffffu, pending, __ffs(waiting) - 1);
+        if (pending == leaf) {
+            leaf_eval(sv, leaf, p, best, cnt);
+            pending = -1;
+        }
+    }
+    return best;
+}
+
 // dist_mat for a whole warp (all 32 lanes call it; lanes with !active only
 // take part in the votes). Each active lane runs its own near-first BVH
 // traversal with the reference's pruning, but leaves are evaluated in
@@ -418,6 +472,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         return best;
     }
     if (sv.n_nodes == 0) return best;
+    if (sv.n_nodes == 3) return dist_mat_warp3(sv, p, active, best, cnt);
     uint32_t* const stack = sv.stk;
     float* const stackd = sv.stkd;
     const int stride = sv.stk_stride;
@@ -472,15 +527,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         const bool shared = sv.n_nodes <= 7 || 2 * __popc(__ballot_sync(0xffffffffu, pending == leaf)) >=
                                                    __popc(waiting);
         if (pending >= 0 && (pending == leaf || !shared)) {
-            const DNode nd = sv.nodes[pending];
-            for (int k = nd.link; k < nd.link + nd.count; ++k) {
-                const DObject o = sv.objs[k];
-                float d = obj_dist(sv, o, p, cnt);
-                if (d < best.d) {
-                    best.d = d;
-                    best.mat = o.mat;
-                }
-            }
+            leaf_eval(sv, pending, p, best, cnt);
             pending = -1;
         }
     }
