@@ -441,7 +441,7 @@ __device__ __forceinline__ DistHit dist_mat_warp3(const SceneView& sv, V p, bool
 // reaches a leaf that passes the AABB test; then, once every lane has either
 // found one or finished, either the lanes sharing the first waiting lane's
 // leaf evaluate it together (the primitive code runs converged) or, in trees
-// of more than four leaves when fewer than half of the waiting lanes share
+// of more than four leaves when fewer than 7/8 of the waiting lanes share
 // that leaf, every waiting lane evaluates its own leaf in the same round
 // (lanes at different leaves then diverge only by primitive kind, instead of
 // waiting a round per leaf). A lane's sequence of node
@@ -522,10 +522,10 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         const int leaf = __shfl_sync(0xffffffffu, pending, __ffs(waiting) - 1);
         // Trees of at most four leaves: one leaf per round, converged. Larger
         // trees: the first waiting lane's leaf is evaluated alone when at
-        // least half the waiting lanes share it; otherwise every waiting lane
-        // evaluates its own leaf in this round.
-        const bool shared = sv.n_nodes <= 7 || 2 * __popc(__ballot_sync(0xffffffffu, pending == leaf)) >=
-                                                   __popc(waiting);
+        // least 7/8 of the waiting lanes share it; otherwise every waiting
+        // lane evaluates its own leaf in this round.
+        const bool shared = sv.n_nodes <= 7 || 8 * __popc(__ballot_sync(0xffffffffu, pending == leaf)) >=
+                                                   7 * __popc(waiting);
         if (pending >= 0 && (pending == leaf || !shared)) {
             leaf_eval(sv, pending, p, best, cnt);
             pending = -1;
