@@ -138,6 +138,7 @@ struct ifx_ctx {
     DBuf work;
     void* pinned = nullptr;  // upload staging (page-locked)
     size_t pinned_cap = 0;
+    cudaEvent_t pinned_ev = nullptr;  // the last copy out of `pinned`
 
     unsigned long long* work_of(int kernel) {
         return counting ? (unsigned long long*)work.p + (size_t)kernel * IFX_WORK_COUNTERS : nullptr;
@@ -358,6 +359,7 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
     if ((e = cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
     for (cudaEvent_t& ev : ctx->fev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreateWithFlags(&ctx->pinned_ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     if (ensure(ctx, ctx->shsc, 32 * 8) != IFX_OK) return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->work, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8) != IFX_OK ||
         cudaMemsetAsync(ctx->work.p, 0, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8, ctx->st) != cudaSuccess)
@@ -419,6 +421,7 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : ctx->fev)
         if (ev) cudaEventDestroy(ev);
+    if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
     if (ctx->st2) cudaStreamDestroy(ctx->st2);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
@@ -533,7 +536,11 @@ extern "C" int ifx_surfels_upload(ifx_ctx* ctx, uint64_t n, const float* p, cons
     if (n > 2000000ull) return fail(ctx, IFX_ERR_LIMIT, "more than 2000000 surfels");
     CK(cudaSetDevice(ctx->device));
     size_t b = n * sizeof(float4);
-    // Repack into the device layout in pinned staging memory, then copy.
+    // Repack into the device layout in pinned staging memory, then copy
+    // without waiting: the copies precede, in stream order, every kernel that
+    // reads the surfels, and the next upload waits for them before it
+    // rewrites the staging memory.
+    CK(cudaEventSynchronize(ctx->pinned_ev));
     if (ctx->pinned_cap < 3 * b) {
         if (ctx->pinned) cudaFreeHost(ctx->pinned);
         ctx->pinned = nullptr;
@@ -563,7 +570,7 @@ extern "C" int ifx_surfels_upload(ifx_ctx* ctx, uint64_t n, const float* p, cons
         CK(cudaMemsetAsync(ctx->sirr.p, 0, b, ctx->st));
         CK(cudaMemsetAsync(ctx->srad.p, 0, b, ctx->st));
     }
-    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaEventRecord(ctx->pinned_ev, ctx->st));
     ctx->n = (uint32_t)n;
     ctx->has_transfer = false;
     ctx->has_grid = false;
