@@ -185,9 +185,9 @@ class L2Flusher:
         self.torch.cuda.synchronize()
 
 
-def fused_frame(ctx, cfg, srgb, cluster_res=8):
+def fused_frame(ctx, cfg, srgb, cluster_res=8, out_srgb=None):
     return ctx.frame(cfg.width, cfg.height, "beauty", cluster_res=cluster_res, max_bounces=cfg.bounces,
-                     linear=False, srgb=srgb)
+                     linear=False, srgb=srgb, out_srgb=out_srgb)
 
 
 def frame(ctx, cfg, cluster_res=8):
@@ -268,7 +268,7 @@ def run_ours(args, world, rank, local) -> dict | None:
     barrier(world)
 
     # End to end through the C ABI with host buffers: scene + surfels in,
-    # encoded image out, every step.
+    # encoded image out (into one host array the caller reuses), every step.
     e2e_ms, e2e_evals = 0.0, 0
     img = np.zeros((cfg.height, cfg.width, 3), np.uint8)
     h2d = None
@@ -277,7 +277,7 @@ def run_ours(args, world, rank, local) -> dict | None:
         ctx.timer_start()
         ctx.upload(scene)
         ctx.upload_surfels(surf["p"], surf["n"], surf["albedo"], surf["area"])
-        f2 = fused_frame(ctx, cfg, srgb=True)
+        f2 = fused_frame(ctx, cfg, srgb=True, out_srgb=img)
         ms = ctx.timer_stop()
         if i >= args.warmup:
             e2e_ms += ms

@@ -302,6 +302,17 @@ def load(path: str) -> Scene:
         return parse(f.read())
 
 
+def _out(buf, shape, dtype, want: bool):
+    """The caller's output array (checked: C-contiguous, shape, dtype), a new
+    one, or None."""
+    if buf is not None:
+        if buf.shape != shape or buf.dtype != dtype or not buf.flags["C_CONTIGUOUS"] or not buf.flags["WRITEABLE"]:
+            raise ValueError(f"output array must be a writeable C-contiguous {np.dtype(dtype).name} array of "
+                             f"shape {shape}")
+        return buf
+    return np.zeros(shape, dtype) if want else None
+
+
 def camera(pos, look, up=(0.0, 1.0, 0.0), fov=40.0) -> _Camera:
     c = _Camera()
     c.pos[:] = pos
@@ -467,32 +478,34 @@ class Context:
         self._check(lib().ifx_grid_build(self._h, radius), "grid build")
 
     def render_frame(self, width: int, height: int, mode="beauty", cam=None, exposure: float | None = None,
-                     linear: bool = True, srgb: bool = True):
+                     linear: bool = True, srgb: bool = True, out_linear=None, out_srgb=None):
         """render_frame + Film::encode. Returns (linear f32 HxWx3 | None, u8 HxWx3 | None, evals)."""
         m = MODES[mode] if isinstance(mode, str) else int(mode)
         if exposure is None:
             exposure = self.scene.cfg.exposure if self.scene is not None else 1.0
-        lin = np.zeros((height, width, 3), np.float32) if linear else None
-        s8 = np.zeros((height, width, 3), np.uint8) if srgb else None
+        lin = _out(out_linear, (height, width, 3), np.float32, linear)
+        s8 = _out(out_srgb, (height, width, 3), np.uint8, srgb)
         e = C.c_uint64()
         self._check(lib().ifx_render_frame(self._h, C.byref(cam) if cam is not None else None, m, width, height,
                                            exposure, _ptr(lin), _ptr(s8), C.byref(e)), "render_frame")
         return lin, s8, e.value
 
     def frame(self, width: int, height: int, mode="beauty", cluster_res: int = 8, max_bounces: int | None = None,
-              cam=None, exposure: float | None = None, linear: bool = True, srgb: bool = True) -> dict:
+              cam=None, exposure: float | None = None, linear: bool = True, srgb: bool = True, out_linear=None,
+              out_srgb=None) -> dict:
         """The transfer build, light_surfels, solve, grid and render_frame in
         one call, the GI-independent shading passes overlapped with the GI
         stages. Returns dict(linear, srgb, transfer, light_evals, solve,
-        shade_evals, ms_frame)."""
+        shade_evals, ms_frame). `out_linear` / `out_srgb` (optional) are
+        arrays to fill instead of new ones, e.g. reused across frames."""
         m = MODES[mode] if isinstance(mode, str) else int(mode)
         cfg = self.scene.cfg if self.scene is not None else None
         if exposure is None:
             exposure = cfg.exposure if cfg is not None else 1.0
         if max_bounces is None:
             max_bounces = cfg.bounces if cfg is not None else 16
-        lin = np.zeros((height, width, 3), np.float32) if linear else None
-        s8 = np.zeros((height, width, 3), np.uint8) if srgb else None
+        lin = _out(out_linear, (height, width, 3), np.float32, linear)
+        s8 = _out(out_srgb, (height, width, 3), np.uint8, srgb)
         fi = _FrameInfo()
         self._check(lib().ifx_frame(self._h, cluster_res, max_bounces, C.byref(cam) if cam is not None else None, m,
                                     width, height, exposure, _ptr(lin), _ptr(s8), C.byref(fi)), "frame")
@@ -506,12 +519,12 @@ class Context:
                     shade_evals=fi.shade_evals, ms_frame=fi.ms_frame)
 
     def render_reference(self, width: int, height: int, spp: int = 512, cam=None, exposure: float | None = None,
-                         linear: bool = True, srgb: bool = True):
+                         linear: bool = True, srgb: bool = True, out_linear=None, out_srgb=None):
         """--mode reference: the path tracer of reference.rs. Returns (linear | None, u8 | None)."""
         if exposure is None:
             exposure = self.scene.cfg.exposure if self.scene is not None else 1.0
-        lin = np.zeros((height, width, 3), np.float32) if linear else None
-        s8 = np.zeros((height, width, 3), np.uint8) if srgb else None
+        lin = _out(out_linear, (height, width, 3), np.float32, linear)
+        s8 = _out(out_srgb, (height, width, 3), np.uint8, srgb)
         self._check(lib().ifx_render_reference(self._h, C.byref(cam) if cam is not None else None, width, height, spp,
                                                exposure, _ptr(lin), _ptr(s8)), "render_reference")
         return lin, s8

@@ -130,3 +130,24 @@ def test_fused_frame_rejects_bad_calls():
         assert lin.tobytes() == f["linear"].tobytes() and ev == f["shade_evals"]
     finally:
         c.close()
+
+
+def test_caller_output_arrays(ctx):
+    """Outputs written into caller arrays equal freshly allocated ones; wrong
+    shapes or types are refused before any device work."""
+    s = ifx.parse(scene_src("cornell"))
+    ctx.upload(s)
+    ctx.generate(2000)
+    a = ctx.frame(24, 16)
+    lin = np.full((16, 24, 3), -1.0, np.float32)
+    s8 = np.full((16, 24, 3), 7, np.uint8)
+    b = ctx.frame(24, 16, out_linear=lin, out_srgb=s8)
+    assert b["linear"] is lin and b["srgb"] is s8
+    assert lin.tobytes() == a["linear"].tobytes() and s8.tobytes() == a["srgb"].tobytes()
+    r8 = np.zeros((16, 24, 3), np.uint8)
+    _, got, _ = ctx.render_frame(24, 16, out_srgb=r8)
+    assert got is r8 and r8.tobytes() == a["srgb"].tobytes()
+    for bad in (np.zeros((16, 24, 3), np.float32), np.zeros((24, 16, 3), np.uint8),
+                np.zeros((16, 24, 6), np.uint8)[:, :, :3]):
+        with pytest.raises(ValueError):
+            ctx.frame(24, 16, out_srgb=bad)
