@@ -98,6 +98,7 @@ struct ifx_ctx {
     // film
     DBuf film, out8;
     DBuf path_sincos;  // (sinf, cosf) of the path tracer's 2^24 sampler angles
+    DBuf lff, lvis, lq, lsc;  // light stage: per-slot ff and visibility, slot queue, queue length + cursor
     // ifx_frame: the second stream that runs the shading passes beside the
     // GI stages, its scratch (16 cursors, the SDF evaluation counter) and
     // events (fork, join, start and end of its work).
@@ -412,7 +413,7 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->ft, &ctx->ftstarts, &ctx->cid, &ctx->hist, &ctx->dg, &ctx->h_t, &ctx->yv, &ctx->ebar,
                     &ctx->rhobar, &ctx->epart, &ctx->eout, &ctx->d3, &ctx->sell_len, &ctx->sell_perm, &ctx->sell_keys,
                     &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w,
-                    &ctx->path_sincos, &ctx->shsc};
+                    &ctx->path_sincos, &ctx->shsc, &ctx->lff, &ctx->lvis, &ctx->lq, &ctx->lsc};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -1072,6 +1073,44 @@ extern "C" int ifx_transfer_upload(ifx_ctx* ctx, const uint32_t* starts, uint64_
     return IFX_OK;
 }
 
+// solve.rs:27-39 on ctx->st: direct = rad = E and irr = 0 for every
+// surfel, the SDF evaluations added to *evals_dev, per-light factors into
+// `terms` (nullable, n x nl). Few (surfel, light) slots leave most lanes of
+// the GPU idle: there each surfel's marches run as one independent thread
+// (latency-bound, so warp-synchronous rounds would only add waiting); many
+// slots go through a queue to the lane-refilling shadow kernel.
+static int light_surfels_run(ifx_ctx* ctx, unsigned long long* evals_dev, unsigned long long* counts, float* terms) {
+    const uint32_t n = ctx->n;
+    if (n == 0) return IFX_OK;
+    const int nl = (int)(ctx->scene.lights.size() + ctx->scene.sphere_lights.size());
+    const size_t slots = (size_t)n * (size_t)(nl > 0 ? nl : 1);
+    if (slots < kLightSlotsQueued) {
+        launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), n, evals_dev, (uint32_t*)ctx->status.p, counts,
+                             terms);
+        ctx->launches++;
+        CKL();
+        return IFX_OK;
+    }
+    ENSURE(ctx->lff, slots * 4);
+    ENSURE(ctx->lvis, slots * 4);
+    ENSURE(ctx->lq, slots * 4);
+    ENSURE(ctx->lsc, 32);
+    ShadeParams P{};
+    P.blob = ctx->blobref;
+    P.status = (uint32_t*)ctx->status.p;
+    P.nl = nl;
+    P.evals = evals_dev;
+    P.counts = counts;
+    P.q1 = (uint32_t*)ctx->lq.p;
+    P.qlen = (uint32_t*)ctx->lsc.p;  // words 0..3
+    unsigned long long* cursor = (unsigned long long*)ctx->lsc.p + 2;
+    CK(cudaMemsetAsync(ctx->lsc.p, 0, 32, ctx->st));
+    ctx->launches += (uint64_t)launch_light_slots(ctx->st, P, ctx->sarr(), n, (float*)ctx->lff.p,
+                                                  (float*)ctx->lvis.p, terms, cursor);
+    CKL();
+    return IFX_OK;
+}
+
 // --------------------------------------------------------------- solve ---
 extern "C" int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals) {
     if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
@@ -1079,12 +1118,8 @@ extern "C" int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals) {
     unsigned long long* small = (unsigned long long*)ctx->small.p;
     CK(cudaMemsetAsync(small, 0, 8, ctx->st));
     CK(cudaEventRecord(ctx->ev0, ctx->st));
-    if (ctx->n) {
-        launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), ctx->n, small, (uint32_t*)ctx->status.p,
-                             ctx->work_of(IFX_KERNEL_LIGHT));
-        ctx->launches++;
-        CKL();
-    }
+    int r0 = light_surfels_run(ctx, small, ctx->work_of(IFX_KERNEL_LIGHT), nullptr);
+    if (r0) return r0;
     CK(cudaEventRecord(ctx->ev1, ctx->st));
     unsigned long long e = 0;
     CK(cudaMemcpyAsync(&e, small, 8, cudaMemcpyDeviceToHost, ctx->st));
@@ -1652,11 +1687,9 @@ extern "C" int ifx_diff_setup(ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, u
     // 1. Each surfel's light factors (with direct = rad = E as a side effect).
     ENSURE(ctx->dterms, (size_t)n * (nl ? nl : 1) * 4);
     unsigned long long* small = (unsigned long long*)ctx->small.p;
-    launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), n, small, (uint32_t*)ctx->status.p, nullptr,
-                         (float*)ctx->dterms.p);
-    ctx->launches++;
-    CKL();
-    int r = check_status(ctx);
+    int r = light_surfels_run(ctx, small, nullptr, (float*)ctx->dterms.p);
+    if (r) return r;
+    r = check_status(ctx);
     if (r) return r;
     // 2. Gather grid and 3. the frame's hits, form factors and visibilities.
     if ((r = ifx_grid_build(ctx, 0.0f))) return r;
@@ -1969,12 +2002,8 @@ extern "C" int ifx_multiscene_add(ifx_multiscene* ms, ifx_ctx* ctx, const ifx_ca
     if (cudaSetDevice(ctx->device) != cudaSuccess) return msfail(ms, IFX_ERR_CUDA, "cudaSetDevice failed");
     const uint32_t n = ctx->n, nl = ctx->nl;
     int r = ensure(ctx, ctx->dterms, (size_t)n * (nl ? nl : 1) * 4);
-    if (!r) {
-        launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), n, (unsigned long long*)ctx->small.p,
-                             (uint32_t*)ctx->status.p, nullptr, (float*)ctx->dterms.p);
-        ctx->launches++;
-        r = check_status(ctx);
-    }
+    if (!r) r = light_surfels_run(ctx, (unsigned long long*)ctx->small.p, nullptr, (float*)ctx->dterms.p);
+    if (!r) r = check_status(ctx);
     if (!r) r = ifx_grid_build(ctx, 0.0f);
     ShadeParams P{};
     if (!r)

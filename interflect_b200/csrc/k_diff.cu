@@ -20,8 +20,8 @@
 namespace ifx {
 
 // ----------------------------------------------------------- forward ----
-// E_i = sum_l (rho_i * e_l) * a_il over the lights direct_diffuse does not
-// skip, in light order: the operations of k_light_surfels' light loop with
+// E_i = sum_l (rho_i * e_l) * a_il over the lights the light stage does not
+// skip, in light order: the operations of the light stage's light loop with
 // the stored factors, so the result is bit-identical to it.
 __global__ void k_relight(const float4* albedo, const float* terms, const float4* emit, int nl, uint32_t n,
                           float4* direct, float4* rad, float4* irr) {

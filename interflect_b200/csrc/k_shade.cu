@@ -324,6 +324,77 @@ int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev, int par
     return ((part & kShadeFront) ? (p.has_gi ? 6 : 3) : 0) + ((part & kShadeCompose) ? 1 : 0);
 }
 
+// ---------------------------------------------------------------------------
+// solve.rs:27-39 (light_surfels) as three passes over (surfel, light) slots:
+// k_light_setup stores each slot's form factor (shade.rs:60-73) and queues
+// the slots that pass the 1e-6 cut; k_shadow marches their cones (the same
+// march, origin offset and end as the light stage's); k_light_compose sums
+// the lights per surfel in the reference's order. Slot = surfel * nl + light
+// (quad lights, then sphere lights).
+template <class C>
+__global__ void __launch_bounds__(128) k_light_setup(ShadeParams P, const float4* sp, const float4* sn, uint32_t n,
+                                                     float* ff_out) {
+    IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
+    C cnt;
+    const int nl = P.nl;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V p = mk4(sp[i]), nn = mk4(sn[i]);
+        V tan, bit;
+        frame(nn, tan, bit);
+        for (int l = 0; l < nl; ++l) {
+            const float ff = light_ff(sv, l, p, nn, tan, bit, cnt);
+            const uint32_t slot = i * (uint32_t)nl + (uint32_t)l;
+            ff_out[slot] = ff;
+            if (!(ff <= 1e-6f)) {  // shade.rs:65: a light is skipped when ff <= 1e-6
+                cnt.add(CN_LIGHT);
+                enqueue(P.q1, &P.qlen[0], slot);
+            }
+        }
+    }
+    if constexpr (sizeof(C) > 1) cnt.flush(P.counts);
+}
+
+__global__ void __launch_bounds__(128) k_light_compose(ShadeParams P, SurfelArrays s, uint32_t n, const float* ff,
+                                                       const float* vis, float* terms) {
+    IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
+    const int nl = P.nl;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V albedo = mk4(s.albedo[i]);
+        V out{0.0f, 0.0f, 0.0f};
+        for (int l = 0; l < nl; ++l) {
+            const size_t slot = (size_t)i * nl + l;
+            if (terms) terms[slot] = -1.0f;
+            const float f = ff[slot];
+            if (f <= 1e-6f) continue;
+            const float v = vis[slot];
+            if (v <= 1e-4f) continue;
+            const float* e = l < sv.n_lights ? sv.lights[l].emit : sv.slights[l - sv.n_lights].emit;
+            out = out + albedo * V{e[0], e[1], e[2]} * (f * v);
+            if (terms) terms[slot] = f * v;
+        }
+        s.direct[i] = f4(out, 0.0f);
+        s.rad[i] = f4(out, 0.0f);
+        s.irr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+int launch_light_slots(cudaStream_t st, const ShadeParams& p, const SurfelArrays& s, uint32_t n, float* ff,
+                       float* vis, float* terms, unsigned long long* cursor) {
+    const size_t sm = blob_smem(p.blob, 128);
+    const unsigned long long slots = (unsigned long long)n * (unsigned long long)(p.nl > 0 ? p.nl : 1);
+    if (p.counts) {
+        k_light_setup<Counts><<<grid_for(n, 128, 16), 128, sm, st>>>(p, s.p, s.n, n, ff);
+        k_shadow<Counts><<<persistent_grid(k_shadow<Counts>, 128, sm, slots), 128, sm, st>>>(
+            p, s.p, s.n, p.q1, &p.qlen[0], vis, cursor);
+    } else {
+        k_light_setup<NoCount><<<grid_for(n, 128, 16), 128, sm, st>>>(p, s.p, s.n, n, ff);
+        k_shadow<NoCount><<<persistent_grid(k_shadow<NoCount>, 128, sm, slots), 128, sm, st>>>(
+            p, s.p, s.n, p.q1, &p.qlen[0], vis, cursor);
+    }
+    k_light_compose<<<grid_for(n, 128, 16), 128, sm, st>>>(p, s, n, ff, vis, terms);
+    return 3;
+}
+
 int launch_compose(cudaStream_t st, const ShadeParams& p) {
     const size_t sm = blob_smem(p.blob, 128);
     ShadeParams q = p;
@@ -345,6 +416,9 @@ static void configure_one(int max_dyn_smem) {
 void configure_shade_kernels(int max_dyn_smem) {
     configure_one<NoCount>(max_dyn_smem);
     configure_one<Counts>(max_dyn_smem);
+    cudaFuncSetAttribute(k_light_setup<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_light_setup<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_light_compose, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }
 
 }  // namespace ifx

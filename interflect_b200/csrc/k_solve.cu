@@ -1,5 +1,6 @@
-// Direct light on surfels (solve.rs:27-39) and the Jacobi bounce solve
-// (solve.rs:47-108). The bounce loop runs without host round trips: every
+// Direct light on surfels (solve.rs:27-39; for many (surfel, light) slots
+// the light stage uses launch_light_slots in k_shade.cu instead) and the
+// Jacobi bounce solve (solve.rs:47-108). The bounce loop runs without host round trips: every
 // bounce kernel first reads a device-side `done` flag, so the host enqueues
 // max_bounces bounces at once and the ones after convergence return
 // immediately.

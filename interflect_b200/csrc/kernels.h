@@ -130,8 +130,12 @@ struct SolveCtl {
     uint32_t residual_bits;  // max |delta| of the bounce in progress (non-negative f32 bits)
     uint32_t last_residual;  // residual of the last completed bounce
 };
+// solve.rs:27-39 with one thread per surfel walking its lights (k_solve.cu);
 // terms (nullable): n x nl, each surfel's per-light factor ff * vis (-1 where
-// the light is skipped), for the differentiable relight.
+// the light is skipped), for the differentiable relight. The light stage uses
+// it below kLightSlotsQueued (surfel, light) slots and launch_light_slots
+// from there on; both compute the same values in the same order.
+static constexpr uint64_t kLightSlotsQueued = 32768;
 void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_t n, unsigned long long* evals,
                           uint32_t* status, unsigned long long* counts = nullptr, float* terms = nullptr);
 // The transfer in sliced-ELL form (k_solve.cu): rows sorted by link count
@@ -218,6 +222,14 @@ int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev, int par
 // k_compose alone over the hits, form factors and visibilities a previous
 // launch_shade with the same parameters left in the wavefront buffers.
 int launch_compose(cudaStream_t st, const ShadeParams& p);
+// solve.rs:27-39 over (surfel, light) slots (k_shade.cu): form factors into
+// ff, the queued slots' cone visibilities into vis (k_shadow, with p.q1 /
+// p.qlen[0] as the queue and `cursor` its position, both zeroed by the
+// caller), then direct = rad = E and irr = 0 per surfel, and terms (nullable,
+// n x nl) = ff * vis or -1. Uses p.blob, p.status, p.nl, p.evals (SDF
+// evaluations added), p.counts. Returns the kernels launched.
+int launch_light_slots(cudaStream_t st, const ShadeParams& p, const SurfelArrays& s, uint32_t n, float* ff,
+                       float* vis, float* terms, unsigned long long* cursor);
 
 // ---- differentiation (k_diff.cu) ----
 // Pixel flags shared with k_shade.cu (hn1.w / hn2.w): hit, done, emitter.

@@ -107,7 +107,7 @@ def test_transfer_parity(ctx, name, target, res):
     assert abs(gi.mean_row_sum - oi["mean_row_sum"]) <= REL * abs(oi["mean_row_sum"])
 
 
-@pytest.mark.parametrize("name,target", [("product", None), ("cornell", 6000)])
+@pytest.mark.parametrize("name,target", [("product", None), ("cornell", 6000), ("product", 30000)])
 def test_light_and_solve_parity(ctx, name, target):
     """solve::light_surfels and solve::solve on the same surfels and the same
     transfer matrix: bounce count exact, radiosities within 1e-4."""
@@ -118,6 +118,8 @@ def test_light_and_solve_parity(ctx, name, target):
     o.build_clusters(8)
     oi = o.build_transfer()
     ctx.build(8)
+    # product at 30000 requested: 18,146 surfels x 2 lights, past the
+    # 32,768 (surfel, light) slots from which the light stage runs queued.
     ge = ctx.light_surfels()
     oe = o.light_surfels()
     assert ge == oe
