@@ -99,6 +99,7 @@ struct ifx_ctx {
     DBuf film, out8;
     DBuf path_sincos;  // (sinf, cosf) of the path tracer's 2^24 sampler angles
     DBuf lff, lvis, lq, lsc;  // light stage: per-slot ff and visibility, slot queue, queue length + cursor
+    DBuf vkey, vkey_alt, vval, vval_alt;  // the visibility queue's order (sort keys, candidate indices)
     // ifx_frame: the second stream that runs the shading passes beside the
     // GI stages, its scratch (16 cursors, the SDF evaluation counter) and
     // events (fork, join, start and end of its work).
@@ -413,7 +414,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->ft, &ctx->ftstarts, &ctx->cid, &ctx->hist, &ctx->dg, &ctx->h_t, &ctx->yv, &ctx->ebar,
                     &ctx->rhobar, &ctx->epart, &ctx->eout, &ctx->d3, &ctx->sell_len, &ctx->sell_perm, &ctx->sell_keys,
                     &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w,
-                    &ctx->path_sincos, &ctx->shsc, &ctx->lff, &ctx->lvis, &ctx->lq, &ctx->lsc};
+                    &ctx->path_sincos, &ctx->shsc, &ctx->lff, &ctx->lvis, &ctx->lq, &ctx->lsc,
+                    &ctx->vkey, &ctx->vkey_alt, &ctx->vval, &ctx->vval_alt};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -906,13 +908,39 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     ctx->launches++;
     CKL();
 
+    // The order the visibility queue walks: a stable sort of the candidates
+    // by (target cluster, source surfel's cluster), so that warps march
+    // nearly parallel cones; results still land in candidate order.
+    const uint32_t* vorder = nullptr;
+    if (ncand > 1 && ncand <= 0x7fffffffull) {
+        ENSURE(ctx->cid, (size_t)n * 4);
+        CK(cudaMemsetAsync(ctx->cid.p, 0xff, (size_t)n * 4, ctx->st));
+        ctx->launches += (uint64_t)launch_cluster_ids(ctx->st, (const uint2*)ctx->crange.p,
+                                                      (const uint32_t*)ctx->members.p, nc, (uint32_t*)ctx->cid.p);
+        ENSURE(ctx->vkey, ncand * 8);
+        ENSURE(ctx->vkey_alt, ncand * 8);
+        ENSURE(ctx->vval, ncand * 4);
+        ENSURE(ctx->vval_alt, ncand * 4);
+        unsigned long long *kin = (unsigned long long*)ctx->vkey.p, *kout = (unsigned long long*)ctx->vkey_alt.p;
+        uint32_t *vin = (uint32_t*)ctx->vval.p, *vout = (uint32_t*)ctx->vval_alt.p;
+        ctx->launches += (uint64_t)launch_vis_keys(ctx->st, ncand, (const uint32_t*)ctx->cand_c.p,
+                                                   (const uint32_t*)ctx->cand_row.p, (const uint32_t*)ctx->cid.p,
+                                                   nc, kin, vin);
+        const unsigned long long kmax = (unsigned long long)nc * (nc + 1ull) + nc;
+        int end_bit = 1;
+        while (end_bit < 64 && (kmax >> end_bit) != 0) ++end_bit;
+        CUB([&](void* t, size_t& b) {
+            return cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int)ncand, 0, end_bit, ctx->st);
+        });
+        vorder = vout;
+    }
     // Visibility and closure (persistent kernels; cursors start at zero).
     ENSURE(ctx->clo, (size_t)n * 16 * 2);
     unsigned long long* cur = (unsigned long long*)ctx->qcur.p;
     CK(cudaMemsetAsync(cur, 0, 16 * 8, ctx->st));
     CK(cudaEventRecord(ctx->kv0, ctx->st));
     launch_visibility(ctx->st, ctx->blobref, ctx->sc, sp, sn, cp, cn, (const uint32_t*)ctx->cand_c.p,
-                      (const uint32_t*)ctx->cand_row.p, ncand, (float*)ctx->cand_vis.p,
+                      (const uint32_t*)ctx->cand_row.p, vorder, ncand, (float*)ctx->cand_vis.p,
                       (uint8_t*)ctx->cand_steps.p, status, ctx->work_of(IFX_KERNEL_VISIBILITY), &cur[0]);
     if (ncand) ctx->launches++;
     CKL();

@@ -73,13 +73,17 @@ __global__ void __launch_bounds__(256) k_pair_fill(const float4* sp, const float
 // formfactor.rs:194-205: the visibility cone of one candidate pair.
 // Persistent: each lane marches one candidate's cone one SDF query per
 // iteration and takes a new candidate from its warp's queue when the cone
-// ends, so a warp stays full however uneven the cones' lengths are.
+// ends, so a warp stays full however uneven the cones' lengths are. The
+// queue walks `order` (nullable: candidate order), a permutation grouping
+// candidates by target cluster and then by the source surfel's cluster, so
+// that a warp marches nearly parallel cones from neighbouring surfels; every
+// result is written to its candidate's own slot.
 template <class C>
 __global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc, const float4* sp,
                                                      const float4* sn, const float4* cp, const float4* cn,
                                                      const uint32_t* cand_c, const uint32_t* cand_row,
-                                                     unsigned long long ncand, float* cand_vis,
-                                                     uint8_t* cand_steps, uint32_t* status,
+                                                     const uint32_t* order, unsigned long long ncand,
+                                                     float* cand_vis, uint8_t* cand_steps, uint32_t* status,
                                                      unsigned long long* counts, unsigned long long* cursor) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
     C cnt;
@@ -88,8 +92,9 @@ __global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc
     uint32_t item = ~0u;
     ShadowRay ray{};
     while (true) {
-        const uint32_t got = q.refill(item == ~0u, ncand, cursor);
+        uint32_t got = q.refill(item == ~0u, ncand, cursor);
         if (got != ~0u) {
+            if (order) got = order[got];
             const uint32_t row = cand_row[got], c = cand_c[got];
             const V p = mk4(__ldg(&sp[row])), nn = mk4(__ldg(&sn[row]));
             const float4 cpc = __ldg(&cp[c]), cnc = __ldg(&cn[c]);
@@ -305,16 +310,36 @@ void launch_pair_fill(cudaStream_t st, const float4* sp, const float4* sn, uint3
 }
 void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
                        const float4* cp, const float4* cn, const uint32_t* cand_c, const uint32_t* cand_row,
-                       unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status,
-                       unsigned long long* counts, unsigned long long* cursor) {
+                       const uint32_t* order, unsigned long long ncand, float* cand_vis, uint8_t* cand_steps,
+                       uint32_t* status, unsigned long long* counts, unsigned long long* cursor) {
     if (ncand == 0) return;
     const size_t sm = blob_smem(blob, 128);
     if (counts)
         k_visibility<Counts><<<persistent_grid(k_visibility<Counts>, 128, sm, ncand), 128, sm, st>>>(
-            blob, sc, sp, sn, cp, cn, cand_c, cand_row, ncand, cand_vis, cand_steps, status, counts, cursor);
+            blob, sc, sp, sn, cp, cn, cand_c, cand_row, order, ncand, cand_vis, cand_steps, status, counts, cursor);
     else
         k_visibility<NoCount><<<persistent_grid(k_visibility<NoCount>, 128, sm, ncand), 128, sm, st>>>(
-            blob, sc, sp, sn, cp, cn, cand_c, cand_row, ncand, cand_vis, cand_steps, status, nullptr, cursor);
+            blob, sc, sp, sn, cp, cn, cand_c, cand_row, order, ncand, cand_vis, cand_steps, status, nullptr,
+            cursor);
+}
+
+// Sort keys of the visibility order: target cluster, then the source
+// surfel's cluster (nc when it has none); values: candidate indices.
+__global__ void k_vis_keys(unsigned long long ncand, const uint32_t* cand_c, const uint32_t* cand_row,
+                           const uint32_t* cid, uint32_t nc, unsigned long long* keys, uint32_t* vals) {
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < ncand; k += stride) {
+        const uint32_t src = cid[cand_row[k]];
+        keys[k] = (unsigned long long)cand_c[k] * (nc + 1ull) + (src < nc ? src : nc);
+        vals[k] = (uint32_t)k;
+    }
+}
+
+int launch_vis_keys(cudaStream_t st, unsigned long long ncand, const uint32_t* cand_c, const uint32_t* cand_row,
+                    const uint32_t* cid, uint32_t nc, unsigned long long* keys, uint32_t* vals) {
+    if (ncand == 0) return 0;
+    k_vis_keys<<<grid_for(ncand, 256), 256, 0, st>>>(ncand, cand_c, cand_row, cid, nc, keys, vals);
+    return 1;
 }
 void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
                     uint32_t n, uint16_t* clo, uint32_t* status, unsigned long long* counts,

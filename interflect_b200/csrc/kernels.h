@@ -103,10 +103,15 @@ void launch_pair_count(cudaStream_t st, const float4* sp, const float4* sn, uint
 void launch_pair_fill(cudaStream_t st, const float4* sp, const float4* sn, uint32_t n, const float4* cp,
                       const float4* cn, uint32_t nc, const unsigned long long* cand_off, uint32_t* cand_c,
                       float* cand_ff, uint32_t* cand_row);
+// `order` (nullable): the permutation of candidates the queue walks.
 void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
                        const float4* cp, const float4* cn, const uint32_t* cand_c, const uint32_t* cand_row,
-                       unsigned long long ncand, float* cand_vis, uint8_t* cand_steps, uint32_t* status,
-                       unsigned long long* counts, unsigned long long* cursor);
+                       const uint32_t* order, unsigned long long ncand, float* cand_vis, uint8_t* cand_steps,
+                       uint32_t* status, unsigned long long* counts, unsigned long long* cursor);
+// Keys (target cluster * (nc + 1) + source cluster) and candidate indices
+// for the stable sort that gives launch_visibility its order.
+int launch_vis_keys(cudaStream_t st, unsigned long long ncand, const uint32_t* cand_c, const uint32_t* cand_row,
+                    const uint32_t* cid, uint32_t nc, unsigned long long* keys, uint32_t* vals);
 // clo: per (row, ray) slot (open << 8) | steps, n * 16 entries.
 void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
                     uint32_t n, uint16_t* clo, uint32_t* status, unsigned long long* counts,
