@@ -100,6 +100,7 @@ struct ifx_ctx {
     DBuf path_sincos;  // (sinf, cosf) of the path tracer's 2^24 sampler angles
     DBuf lff, lvis, lq, lsc;  // light stage: per-slot ff and visibility, slot queue, queue length + cursor
     DBuf vkey, vkey_alt, vval, vval_alt;  // the visibility queue's order (sort keys, candidate indices)
+    DBuf ckey, ckey_alt, cval, cval_alt;  // the closure queue's order (sort keys, item indices)
     // ifx_frame: the second stream that runs the shading passes beside the
     // GI stages, its scratch (16 cursors, the SDF evaluation counter) and
     // events (fork, join, start and end of its work).
@@ -415,7 +416,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->rhobar, &ctx->epart, &ctx->eout, &ctx->d3, &ctx->sell_len, &ctx->sell_perm, &ctx->sell_keys,
                     &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w,
                     &ctx->path_sincos, &ctx->shsc, &ctx->lff, &ctx->lvis, &ctx->lq, &ctx->lsc,
-                    &ctx->vkey, &ctx->vkey_alt, &ctx->vval, &ctx->vval_alt};
+                    &ctx->vkey, &ctx->vkey_alt, &ctx->vval, &ctx->vval_alt, &ctx->ckey, &ctx->ckey_alt,
+                    &ctx->cval, &ctx->cval_alt};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -908,15 +910,34 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     ctx->launches++;
     CKL();
 
-    // The order the visibility queue walks: a stable sort of the candidates
-    // by (target cluster, source surfel's cluster), so that warps march
-    // nearly parallel cones; results still land in candidate order.
+    // The orders the visibility and closure queues walk: stable sorts of the
+    // candidates by (target cluster, source surfel's cluster) and of the
+    // hemisphere rays by (surfel's cluster, direction), so that warps march
+    // nearly parallel rays; results still land in their own slots.
+    ENSURE(ctx->cid, (size_t)n * 4);
+    CK(cudaMemsetAsync(ctx->cid.p, 0xff, (size_t)n * 4, ctx->st));
+    ctx->launches += (uint64_t)launch_cluster_ids(ctx->st, (const uint2*)ctx->crange.p,
+                                                  (const uint32_t*)ctx->members.p, nc, (uint32_t*)ctx->cid.p);
+    const uint32_t* corder = nullptr;
+    if (n > 0 && (nc + 1ull) * 16ull <= 0xffffffffull) {
+        const size_t items = (size_t)n * 16;
+        ENSURE(ctx->ckey, items * 4);
+        ENSURE(ctx->ckey_alt, items * 4);
+        ENSURE(ctx->cval, items * 4);
+        ENSURE(ctx->cval_alt, items * 4);
+        uint32_t *kin = (uint32_t*)ctx->ckey.p, *kout = (uint32_t*)ctx->ckey_alt.p;
+        uint32_t *vin = (uint32_t*)ctx->cval.p, *vout = (uint32_t*)ctx->cval_alt.p;
+        ctx->launches += (uint64_t)launch_clo_keys(ctx->st, n, (const uint32_t*)ctx->cid.p, nc, kin, vin);
+        const unsigned long long kmax = (nc + 1ull) * 16ull;
+        int end_bit = 1;
+        while (end_bit < 32 && (kmax >> end_bit) != 0) ++end_bit;
+        CUB([&](void* t, size_t& b) {
+            return cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int)items, 0, end_bit, ctx->st);
+        });
+        corder = vout;
+    }
     const uint32_t* vorder = nullptr;
     if (ncand > 1 && ncand <= 0x7fffffffull) {
-        ENSURE(ctx->cid, (size_t)n * 4);
-        CK(cudaMemsetAsync(ctx->cid.p, 0xff, (size_t)n * 4, ctx->st));
-        ctx->launches += (uint64_t)launch_cluster_ids(ctx->st, (const uint2*)ctx->crange.p,
-                                                      (const uint32_t*)ctx->members.p, nc, (uint32_t*)ctx->cid.p);
         ENSURE(ctx->vkey, ncand * 8);
         ENSURE(ctx->vkey_alt, ncand * 8);
         ENSURE(ctx->vval, ncand * 4);
@@ -946,7 +967,7 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     CKL();
     CK(cudaEventRecord(ctx->kv1, ctx->st));
     CK(cudaEventRecord(ctx->kc0, ctx->st));
-    launch_closure(ctx->st, ctx->blobref, ctx->sc, sp, sn, n, (uint16_t*)ctx->clo.p, status,
+    launch_closure(ctx->st, ctx->blobref, ctx->sc, sp, sn, n, corder, (uint16_t*)ctx->clo.p, status,
                    ctx->work_of(IFX_KERNEL_CLOSURE), &cur[1]);
     ctx->launches++;
     CKL();

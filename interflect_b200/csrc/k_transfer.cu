@@ -127,13 +127,17 @@ __global__ void __launch_bounds__(128) k_visibility(BlobRef blob, SceneConsts sc
 
 // trace.rs:165-186: one persistent lane per hemisphere ray (16 per row);
 // each ray's result is written to its own slot as (open << 8) | steps and
-// k_row_finalize reduces the row's 16 slots. A hit's normal is never used
+// k_row_finalize reduces the row's 16 slots. The queue walks `order`
+// (nullable: item order), which groups rays by the row's cluster and then
+// by direction, so a warp marches nearly parallel rays from neighbouring
+// surfels. A hit's normal is never used
 // here, so it is not computed, but its four taps are still counted
 // (trace.rs:48).
 template <class C>
 __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, const float4* sp,
-                                                  const float4* sn, uint32_t n, uint16_t* clo, uint32_t* status,
-                                                  unsigned long long* counts, unsigned long long* cursor) {
+                                                  const float4* sn, uint32_t n, const uint32_t* order, uint16_t* clo,
+                                                  uint32_t* status, unsigned long long* counts,
+                                                  unsigned long long* cursor) {
     IFX_SCENE_PROLOGUE(blob, status, sv);
     C cnt;
     const unsigned long long total = (unsigned long long)n * 16ull;
@@ -142,8 +146,9 @@ __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, c
     uint32_t item = ~0u;
     TraceRay ray{};
     while (true) {
-        const uint32_t got = q.refill(item == ~0u, total, cursor);
+        uint32_t got = q.refill(item == ~0u, total, cursor);
         if (got != ~0u) {
+            if (order) got = order[got];
             const uint32_t row = got >> 4, k = got & 15u;
             const V p = mk4(__ldg(&sp[row])), nn = mk4(__ldg(&sn[row]));
             V t, b;
@@ -342,16 +347,33 @@ int launch_vis_keys(cudaStream_t st, unsigned long long ncand, const uint32_t* c
     return 1;
 }
 void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
-                    uint32_t n, uint16_t* clo, uint32_t* status, unsigned long long* counts,
+                    uint32_t n, const uint32_t* order, uint16_t* clo, uint32_t* status, unsigned long long* counts,
                     unsigned long long* cursor) {
     const size_t sm = blob_smem(blob, 128);
     const unsigned long long items = (unsigned long long)n * 16ull;
     if (counts)
         k_closure<Counts><<<persistent_grid(k_closure<Counts>, 128, sm, items), 128, sm, st>>>(
-            blob, sc, sp, sn, n, clo, status, counts, cursor);
+            blob, sc, sp, sn, n, order, clo, status, counts, cursor);
     else
         k_closure<NoCount><<<persistent_grid(k_closure<NoCount>, 128, sm, items), 128, sm, st>>>(
-            blob, sc, sp, sn, n, clo, status, nullptr, cursor);
+            blob, sc, sp, sn, n, order, clo, status, nullptr, cursor);
+}
+
+// Sort keys of the closure order: the row's cluster (nc when it has none),
+// then the direction index; values: item indices (row * 16 + direction).
+__global__ void k_clo_keys(uint32_t n, const uint32_t* cid, uint32_t nc, uint32_t* keys, uint32_t* vals) {
+    const uint32_t total = n * 16u;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t c = cid[t >> 4];
+        keys[t] = (c < nc ? c : nc) * 16u + (t & 15u);
+        vals[t] = t;
+    }
+}
+
+int launch_clo_keys(cudaStream_t st, uint32_t n, const uint32_t* cid, uint32_t nc, uint32_t* keys, uint32_t* vals) {
+    if (n == 0) return 0;
+    k_clo_keys<<<grid_for((unsigned long long)n * 16ull, 256), 256, 0, st>>>(n, cid, nc, keys, vals);
+    return 1;
 }
 void launch_row_finalize(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const float* cand_ff,
                          const float* cand_vis, const uint8_t* cand_steps, const uint16_t* clo, uint32_t* row_links,

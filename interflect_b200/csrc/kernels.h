@@ -114,8 +114,11 @@ int launch_vis_keys(cudaStream_t st, unsigned long long ncand, const uint32_t* c
                     const uint32_t* cid, uint32_t nc, unsigned long long* keys, uint32_t* vals);
 // clo: per (row, ray) slot (open << 8) | steps, n * 16 entries.
 void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4* sp, const float4* sn,
-                    uint32_t n, uint16_t* clo, uint32_t* status, unsigned long long* counts,
+                    uint32_t n, const uint32_t* order, uint16_t* clo, uint32_t* status, unsigned long long* counts,
                     unsigned long long* cursor);
+// Keys ((row's cluster) * 16 + direction) and item indices for the stable
+// sort that gives launch_closure its order.
+int launch_clo_keys(cudaStream_t st, uint32_t n, const uint32_t* cid, uint32_t nc, uint32_t* keys, uint32_t* vals);
 void launch_row_finalize(cudaStream_t st, uint32_t n, const unsigned long long* cand_off, const float* cand_ff,
                          const float* cand_vis, const uint8_t* cand_steps, const uint16_t* clo, uint32_t* row_links,
                          float* row_scale, float* row_sum, float* row_sky, unsigned long long* row_evals);
