@@ -620,7 +620,10 @@ def run_solve_hbm(args, world, rank, local) -> dict | None:
         return None
     bpb = solve_bytes(L, n, nc)
     gbs = bpb * st.iterations / (t_max / 1e3) / 1e9
-    peak = measured_peaks().get("hbm_gbs", 6650.0)
+    mp = measured_peaks()
+    peak = mp.get("hbm_gbs", 6650.0)
+    peak_src = ("MEASURED_PEAKS.json hbm_gbs (copy bandwidth)" if "hbm_gbs" in mp
+                else "fallback 6650 GB/s (an earlier copy-bandwidth measurement on this pool)")
     traffic = None
     tj = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tj):
@@ -634,7 +637,7 @@ def run_solve_hbm(args, world, rank, local) -> dict | None:
                    "bytes_per_bounce": bpb, "l2": "flushed before each solve; working set 7x the 126 MB L2"},
         "roofline": {"kernel": "k_jacobi_sell + k_cluster_agg", "bound": "hbm", "achieved": gbs, "peak": peak,
                      "unit": "GB/s", "frac": gbs / peak, "traffic": traffic,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"},
+                     "peak_source": peak_src},
         "csr_kernel": {"value": bpb * st.iterations / (csr_max / 1e3) / 1e9, "unit": "GB/s",
                        "ms": csr_max, "bit_identical_to_sliced_ell": same},
         "gpu_launches": 3 * st.iterations * args.steps,
