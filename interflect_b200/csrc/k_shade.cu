@@ -17,6 +17,7 @@
 // fixed by pixel and light, and every float sum is formed in k_compose in
 // the reference's order, so the image is bit-identical across runs.
 #include "shade.cuh"
+#include "pixorder.h"
 
 namespace ifx {
 
@@ -26,8 +27,9 @@ static constexpr uint32_t kFlagEmit = kPixEmit;
 static constexpr uint32_t kMatMask = kPixMatMask;
 
 // ------------------------------------------------------------ kernels ----
-// Camera rays: trace.rs:27-58 from the eye (main.rs:261). hn1 keeps the
-// march's step count in x until k_setup replaces it with the normal.
+// Camera rays: trace.rs:27-58 from the eye (main.rs:261), pixels taken in
+// 8 x 4 tiles (pixorder.h). hn1 keeps the march's step count in x until
+// k_setup replaces it with the normal.
 template <class C>
 __global__ void __launch_bounds__(128) k_primary(ShadeParams P) {
     IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
@@ -41,8 +43,9 @@ __global__ void __launch_bounds__(128) k_primary(ShadeParams P) {
     while (true) {
         const uint32_t got = q.refill(item == ~0u, total, &P.cursors[0]);
         if (got != ~0u) {
-            ray = TraceRay{org, camera_ray(P, got), 1e-3f, P.tmax, 0u};
-            item = got;
+            const uint32_t pix = tile_pixel(got, P.w, P.h);
+            ray = TraceRay{org, camera_ray(P, pix), 1e-3f, P.tmax, 0u};
+            item = pix;
         }
         if (!__any_sync(kFull, item != ~0u)) {
             if (q.empty()) break;
@@ -78,7 +81,8 @@ __global__ void __launch_bounds__(128) k_setup(ShadeParams P) {
     const uint32_t total = P.w * P.h;
     const V org{P.cam.origin[0], P.cam.origin[1], P.cam.origin[2]};
     const bool tonemapped = P.mode <= 2;
-    for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < total; pix += gridDim.x * blockDim.x) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t pix = tile_pixel(t, P.w, P.h);  // the queues then fill in tile order
         const float4 a = P.hp1[pix];
         const float4 b = P.hn1[pix];
         const uint32_t flags = __float_as_uint(b.w);
