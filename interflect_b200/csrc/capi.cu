@@ -2209,7 +2209,10 @@ extern "C" int ifx_multiscene_build(ifx_multiscene* ms, int autotune, int* grid_
         if (!autotune) break;
     }
     if (shapes.empty()) return msfail(ms, IFX_ERR_CUDA, "the packed kernel cannot be made resident");
-    if (!autotune) shapes = {shapes.back()};
+    if (!autotune) {
+        const Shape last = shapes.back();
+        shapes.assign(1, last);
+    }
     float best = 3.4e38f;
     Shape pick = shapes.back();
     if (shapes.size() > 1) {
