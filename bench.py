@@ -7,7 +7,13 @@ reference runs after surfel generation (main.rs:448-475 and 522-534). Surfel
 generation runs once before timing and is reported separately.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2_product] [--no-cpu-baseline]
+                    [--workload c2_product|c2_product_strict|c1_cornell|c3_stress|c4_batch|
+                                c4_multi|c5_diff|solve_hbm|pathtrace]
+                    [--no-cpu-baseline] [--film WxH] [--surfels N]
+
+`c2_product` (the default) times one `ifx_frame` call per step; `--film` and
+`--surfels` shrink a workload for profiling or for a CPU comparison the
+oracle can finish.
 
 N > 1 runs under torchrun as N independent replicas (one process per GPU,
 each rendering its own frame; the path has no cross-GPU exchange), timed on
@@ -866,6 +872,13 @@ def run_reference(args, world, rank) -> dict | None:
         return None
     if args.workload == "pathtrace":
         return run_reference_pathtrace(args, world)
+    if args.workload in ("c4_batch", "c4_multi", "c5_diff", "solve_hbm"):
+        # Batched relighting, packed scenes, gradients and the solve alone have
+        # no CPU entry point in the reference; these lines carry their own
+        # baselines (plain per-RHS / per-scene loops, the forward frame, the
+        # CSR kernel).
+        return {"impl": "reference", "unavailable": f"the reference has no CPU counterpart of the {args.workload} "
+                                                    "workload; its line reports its own baseline"}
     import interflect_b200  # noqa: F401  (scene parsing only)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Oracle
