@@ -191,6 +191,24 @@ class L2Flusher:
         self.torch.cuda.synchronize()
 
 
+L2_NOTE = ("GPU arm: L2 flushed (256 MB write) before every timed step; CPU arm: the oracle on the host cores, "
+           "no flush")
+SURFEL_NOTE = {
+    "c2_product": "200k surfels requested, 55,003 placed: the reference's generator draws min(24 x target, 6M) "
+                  "Halton seeds (surfel.rs:183) and keeps those that pass its Poisson-disc spacing for the "
+                  "requested density, which this scene's surface area allows 55,003 times; links follow "
+                  "(772,534), so the ~2M links a 200k-surfel scene would have are unreachable under the "
+                  "reference algorithm",
+}
+
+
+def workload_config(workload, scene_path, desc, cfg, placed, world) -> dict:
+    """The workload's identity, the same keys and values in both arms."""
+    return {"workload": workload, "scene": scene_path, "description": desc, "film": f"{cfg.width}x{cfg.height}",
+            "surfels_requested": cfg.surfels, "surfels_placed": placed, "max_bounces": cfg.bounces,
+            "cluster_res": 8, "l2": L2_NOTE, "parallelism": f"replicas x{world}"}
+
+
 def fused_frame(ctx, cfg, srgb, cluster_res=8, out_srgb=None):
     return ctx.frame(cfg.width, cfg.height, "beauty", cluster_res=cluster_res, max_bounces=cfg.bounces,
                      linear=False, srgb=srgb, out_srgb=out_srgb)
@@ -329,13 +347,11 @@ def run_ours(args, world, rank, local) -> dict | None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "scene": scene_path, "description": desc,
-                   "film": [cfg.width, cfg.height], "surfels_requested": cfg.surfels, "surfels_placed": placed,
-                   "clusters": info.clusters, "candidates": info.candidates, "links": info.links,
-                   "bounces_run": st.iterations, "max_bounces": cfg.bounces,
-                   "evals_per_frame": evals_total // max(args.steps, 1),
-                   "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}",
-                   "frame": "ifx_frame: GI stages on one stream, GI-free shading passes overlapped on a second"},
+        "config": workload_config(args.workload, scene_path, desc, cfg, placed, world),
+        "workload_stats": {"clusters": info.clusters, "candidates": info.candidates, "links": info.links,
+                           "bounces_run": st.iterations, "evals_per_frame": evals_total // max(args.steps, 1),
+                           "note": SURFEL_NOTE.get(args.workload, "")},
+        "frame": "ifx_frame: GI stages on one stream, GI-free shading passes overlapped on a second",
         "frame_ms": t_max / args.steps,
         "staged_frame_ms": staged_ms / n_staged,
         "stage_ms": {k: statistics.mean(v) for k, v in stage.items()},
@@ -354,7 +370,11 @@ def run_ours(args, world, rank, local) -> dict | None:
         "clocks": clocks,
     }
     if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(src, surf, cfg, args)
+        threads = os.cpu_count() or 1
+        stride, rows_frac = cpu_sample_plan(placed, cfg.width, cfg.height, args)
+        c = cpu_frame(src, surf, cfg, threads, stride=stride, rows_frac=rows_frac)
+        line["cpu_baseline"] = cpu_baseline(c, cfg, threads)
+        line["parity"] = frame_parity(ctx, cfg, c)
     return line
 
 
@@ -733,32 +753,123 @@ def run_diff(args, world, rank, local) -> dict | None:
     }
 
 
-def cpu_frame(src, surf, cfg, threads, rows_frac=1.0):
+def cpu_sample_plan(placed: int, width: int, height: int, args) -> tuple[int, float]:
+    """(row stride of the transfer and light stages, fraction of film rows
+    shaded) for the CPU legs: every row up to 100k surfels and 1080p, else a
+    bounded sample (about 10k surfel rows, about 330k pixels) so that one CPU
+    frame stays within tens of seconds."""
+    stride = args.cpu_stride if args.cpu_stride else max(1, -(-placed // 10000)) if placed > 100000 else 1
+    if args.cpu_rows:
+        rows_frac = args.cpu_rows
+    else:
+        rows_frac = 1.0 if width * height <= 1920 * 1080 else min(1.0, 330000 / (width * height))
+    return stride, rows_frac
+
+
+def cpu_frame(src, surf, cfg, threads, stride=1, rows_frac=1.0):
     """One frame of the oracle (the reference algorithm on the CPU) on the
-    given surfels; shading restricted to the first rows_frac of the rows."""
+    given surfels, stage by stage. With stride > 1 only every stride-th
+    transfer row and surfel light is computed, and with rows_frac < 1 only
+    the first rows of the film are shaded: the sample the rate is taken on.
+    Returns the evaluation counts, the per-stage seconds, the film and the
+    oracle itself (for the parity comparison)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Oracle
     o = Oracle(src, threads=threads)
     o.set_surfels(surf["p"], surf["n"], surf["albedo"], surf["area"])
+    t = {}
     t0 = time.perf_counter()
     o.build_clusters(8)
-    info = o.build_transfer()
-    le = o.light_surfels()
-    o.solve(cfg.bounces)
+    info = o.build_transfer(stride)
+    t["transfer"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    le = o.light_surfels(stride)
+    t["light"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    it, _ = o.solve(cfg.bounces)
+    t["solve"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
     o.build_grid()
+    t["grid"] = time.perf_counter() - t0
     rows = max(1, int(cfg.height * rows_frac))
-    _, se = o.render(cfg.width, cfg.height, "beauty", rows=(0, rows))
-    dt = time.perf_counter() - t0
-    return info["evals"] + le + se, dt, rows
+    t0 = time.perf_counter()
+    film, se = o.render(cfg.width, cfg.height, "beauty", rows=(0, rows))
+    t["shade"] = time.perf_counter() - t0
+    return dict(evals=info["evals"] + le + se, transfer_evals=info["evals"], light_evals=le, shade_evals=se,
+                stage_s=t, dt=sum(t.values()), rows=rows, stride=stride, film=film, info=info, iterations=it,
+                oracle=o)
 
 
-def cpu_baseline(src, surf, cfg, args) -> dict:
-    threads = os.cpu_count() or 1
-    ev, dt, rows = cpu_frame(src, surf, cfg, threads, rows_frac=args.cpu_rows)
-    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"one frame of the same workload on the same surfels, shading rows 0..{rows} of "
-                      f"{cfg.height}; {ev / 1e6:.1f}M SDF evals in {dt:.2f} s",
-            "cpu": cpu_model()}
+def cpu_baseline(c: dict, cfg, threads: int) -> dict:
+    """The CPU leg's line: SDF evaluations per second of the oracle on the
+    host cores over the sample `c` (cpu_frame's result)."""
+    full = c["stride"] == 1 and c["rows"] == cfg.height
+    if full:
+        value = c["evals"] / c["dt"]
+        sample = (f"one frame of the same workload on the same surfels, every transfer row and film row; "
+                  f"{c['evals'] / 1e6:.1f}M SDF evals in {c['dt']:.2f} s")
+    else:
+        # The ray stages' rate on the sample; the solve and grid run in full
+        # on the sampled matrix and are not part of the rate.
+        st = c["stage_s"]
+        ray_s = st["transfer"] + st["light"] + st["shade"]
+        value = c["evals"] / ray_s
+        est = (st["transfer"] + st["light"]) * c["stride"] + st["shade"] * cfg.height / c["rows"]
+        sample = (f"transfer rows and surfel lights i % {c['stride']} == 0 and film rows 0..{c['rows']} of "
+                  f"{cfg.height}: {c['evals'] / 1e6:.1f}M SDF evals in {ray_s:.2f} s of ray stages "
+                  f"(transfer {st['transfer']:.2f} s, light {st['light']:.2f} s, shade {st['shade']:.2f} s); "
+                  f"a whole frame at these rates is about {est:.0f} s")
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample, "cpu": cpu_model(),
+            "stage_s": c["stage_s"]}
+
+
+def frame_parity(ctx, cfg, c: dict) -> dict:
+    """The GPU's frame against the oracle's on the same surfels: link rows of
+    the sampled transfer rows (column indices exact, weights and per-row
+    evaluation counts), direct light of the sampled surfels, and, where the
+    CPU ran the whole frame, the bounce count and every shaded film row."""
+    import numpy as np
+    o = c["oracle"]
+    n = ctx.n_surfels
+    f = ctx.frame(cfg.width, cfg.height, "beauty", cluster_res=8, max_bounces=cfg.bounces, linear=True, srgb=False)
+    gt = ctx.transfer()
+    ot = o.transfer(n, c["info"]["links"])
+    rows = np.arange(0, n, c["stride"])
+    gs, os_ = gt["starts"].astype(np.int64), ot["starts"].astype(np.int64)
+    mism, wmax = 0, 0.0
+    for i in rows:
+        gi_, oi_ = gt["idx"][gs[i]:gs[i + 1]], ot["idx"][os_[i]:os_[i + 1]]
+        if not np.array_equal(gi_, oi_):
+            mism += 1
+            continue
+        if len(gi_):
+            a = gt["w"][gs[i]:gs[i + 1]].astype(np.float64)
+            b = ot["w"][os_[i]:os_[i + 1]].astype(np.float64)
+            wmax = max(wmax, float((np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-6)).max()))
+    gd = ctx.row_diag()
+    evals_equal = bool(np.array_equal(gd["row_evals"][rows], ot["row_evals"][rows]))
+    out = {"rows_compared": int(len(rows)), "link_row_mismatches": int(mism), "link_weight_max_rel": wmax,
+           "row_evals_equal": evals_equal}
+    full = c["stride"] == 1 and c["rows"] == cfg.height
+    if c["stride"] == 1:
+        g, r = ctx.surfels(), o.surfels()
+        e = np.abs(g["direct"].astype(np.float64) - r["direct"]) / np.maximum(
+            np.maximum(np.abs(g["direct"]), np.abs(r["direct"])), 1e-6)
+        out["direct_max_rel"] = float(e.max()) if e.size else 0.0
+        out["bounces_equal"] = f["solve"].iterations == c["iterations"]
+    if full:
+        lin, film = f["linear"].astype(np.float64), c["film"].astype(np.float64)
+        e = np.abs(lin - film) / np.maximum(np.maximum(np.abs(lin), np.abs(film)), 1e-6)
+        out.update({"film_rows_compared": c["rows"], "max_rel": float(e.max()), "rms": float(np.sqrt(np.mean(e ** 2))),
+                    "bit_identical_frac": float(np.mean(f["linear"] == c["film"])),
+                    "evals_equal": f["transfer"].evals + f["light_evals"] + f["shade_evals"] == c["evals"]})
+    else:
+        out["film"] = "not compared: the sampled transfer leaves the CPU solve incomplete"
+    out["tolerance"] = "integers exact, floats within 1e-4 relative"
+    out["ok"] = bool(mism == 0 and wmax <= 1e-4 and evals_equal and out.get("max_rel", 0.0) <= 1e-4
+                     and out.get("direct_max_rel", 0.0) <= 1e-4 and out.get("bounces_equal", True)
+                     and out.get("evals_equal", True))
+    return out
 
 
 def cpu_model() -> str:
@@ -879,7 +990,6 @@ def run_reference(args, world, rank) -> dict | None:
         # CSR kernel).
         return {"impl": "reference", "unavailable": f"the reference has no CPU counterpart of the {args.workload} "
                                                     "workload; its line reports its own baseline"}
-    import interflect_b200  # noqa: F401  (scene parsing only)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Oracle
     scene_path, desc = WORKLOADS[args.workload]
@@ -888,29 +998,39 @@ def run_reference(args, world, rank) -> dict | None:
     threads = os.cpu_count() or 1
     o = Oracle(src, threads=threads)
     cfg_i = o.info()
-    t0 = time.time()
-    placed = o.generate(cfg_i["surfels"])
-    gen_s = time.time() - t0
-    surf = o.surfels()
 
     class Cfg:
-        width, height, bounces = cfg_i["width"], cfg_i["height"], cfg_i["bounces"]
-    total_t, total_ev, rows = 0.0, 0, cfg_i["height"]
+        width, height, bounces, surfels = cfg_i["width"], cfg_i["height"], cfg_i["bounces"], cfg_i["surfels"]
+    if args.film:
+        Cfg.width, Cfg.height = (int(v) for v in args.film.lower().split("x"))
+    if args.surfels:
+        Cfg.surfels = args.surfels
+    t0 = time.time()
+    placed = o.generate(Cfg.surfels)
+    gen_s = time.time() - t0
+    surf = o.surfels()
+    stride, rows_frac = cpu_sample_plan(placed, Cfg.width, Cfg.height, args)
+    total_t, total_ev, last = 0.0, 0, None
     for i in range(args.warmup + args.steps):
-        ev, dt, rows = cpu_frame(src, surf, Cfg, threads, rows_frac=args.cpu_rows)
+        c = cpu_frame(src, surf, Cfg, threads, stride=stride, rows_frac=rows_frac)
+        b = cpu_baseline(c, Cfg, threads)
         if i >= args.warmup:
-            total_t += dt
-            total_ev += ev
+            total_t += c["evals"] / b["value"]
+            total_ev += c["evals"]
+        last = (c, b)
     value = total_ev / total_t
+    c, b = last
+    b["value"] = value
+    b["sample"] = f"{args.steps} timed steps, each " + b["sample"]
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_t / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "scene": scene_path, "description": desc,
-                       "surfels_placed": placed, "film": [cfg_i["width"], cfg_i["height"]]},
+            "config": workload_config(args.workload, scene_path, desc, Cfg, placed, world),
+            "workload_stats": {"clusters": c["info"]["clusters"], "links": c["info"]["links"],
+                               "bounces_run": c["iterations"], "evals_per_step": c["evals"],
+                               "note": SURFEL_NOTE.get(args.workload, "")},
             "surfel_generation_s": gen_s,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} frames on the host cores, shading rows 0..{rows} of "
-                                       f"{cfg_i['height']}", "cpu": cpu_model()},
+            "cpu_baseline": b,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the Rust reference cannot be built in this image (no rustc/cargo); this arm times the "
                     "oracle, a line-by-line C++ restatement of the reference's CPU path, on all host threads"}
@@ -950,7 +1070,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2_product", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-rows", type=float, default=1.0, help="fraction of film rows the CPU legs shade")
+    ap.add_argument("--cpu-rows", type=float, default=None,
+                    help="fraction of film rows the CPU legs shade (default: all up to 1080p, else about 330k pixels)")
+    ap.add_argument("--cpu-stride", type=int, default=None,
+                    help="CPU legs compute transfer rows and surfel lights i %% stride == 0 (default: 1 up to "
+                         "100k surfels, else about 10k rows)")
     ap.add_argument("--film", default=None, help="WxH film override for small profiling cases (e.g. 640x360)")
     ap.add_argument("--surfels", type=int, default=None, help="surfel target override for small profiling cases")
     args = ap.parse_args()
@@ -973,6 +1097,11 @@ def main():
             line = run_ours(args, world, rank, local)
         if line is not None:
             print(json.dumps(line), flush=True)
+            if not line.get("parity", {}).get("ok", True):
+                # A fast frame that differs from the reference algorithm's is
+                # not a result: say so and fail the run.
+                print(f"bench: the GPU frame differs from the oracle's: {line['parity']}", file=sys.stderr)
+                sys.exit(3)
     finally:
         if world > 1:
             import torch.distributed as dist

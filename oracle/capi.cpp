@@ -236,8 +236,16 @@ int orc_get_clusters(orc_ctx* c, float* pnar8, uint32_t* offsets, uint32_t* memb
 
 // Builds the transfer from the clusters of the last orc_build_clusters call.
 // info[0..3]: nc, links, evals, interior rows; *mean_row_sum.
+int orc_build_transfer_sampled(orc_ctx* c, int64_t stride, int64_t* info, float* mean_row_sum);
+
 int orc_build_transfer(orc_ctx* c, int64_t* info, float* mean_row_sum) {
-    uint64_t ev = build_transfer(c->scene, c->surfels, c->clusters, c->transfer, c->threads);
+    return orc_build_transfer_sampled(c, 1, info, mean_row_sum);
+}
+
+// Rows i % stride == 0 only (stride 1: every row); the others stay empty.
+int orc_build_transfer_sampled(orc_ctx* c, int64_t stride, int64_t* info, float* mean_row_sum) {
+    uint64_t ev = build_transfer(c->scene, c->surfels, c->clusters, c->transfer, c->threads,
+                                 (size_t)(stride < 1 ? 1 : stride));
     c->has_transfer = true;
     int64_t interior = 0;
     for (size_t i = 0; i + 1 < c->transfer.starts.size(); ++i)
@@ -278,6 +286,11 @@ int orc_set_transfer(orc_ctx* c, int64_t n, const uint32_t* starts, int64_t link
 }
 
 int64_t orc_light_surfels(orc_ctx* c) { return (int64_t)light_surfels(c->scene, c->surfels, c->threads); }
+
+// Surfels i % stride == 0 only.
+int64_t orc_light_surfels_sampled(orc_ctx* c, int64_t stride) {
+    return (int64_t)light_surfels(c->scene, c->surfels, c->threads, (size_t)(stride < 1 ? 1 : stride));
+}
 
 int orc_solve_ex(orc_ctx* c, uint32_t max_bounces, int fixed, uint32_t* iterations, float* residual);
 

@@ -642,7 +642,7 @@ void build_clusters(const Scene& sc, const Surfels& s, int32_t res, std::vector<
 
 // formfactor.rs:153-277
 uint64_t build_transfer(const Scene& sc, const Surfels& s, std::vector<Cluster> clusters, Transfer& t,
-                        int threads) {
+                        int threads, size_t stride) {
     size_t nc = clusters.size();
     float diag = length(sc.hi - sc.lo);
     size_t N = s.size();
@@ -652,7 +652,9 @@ uint64_t build_transfer(const Scene& sc, const Surfels& s, std::vector<Cluster> 
     t.row_sky.assign(N, 0.0f);
     t.row_evals.assign(N, 0);
     t.cand_count.assign(N, 0);
-    parallel_rows(N, threads, [&](size_t i) {
+    if (stride < 1) stride = 1;
+    parallel_rows((N + stride - 1) / stride, threads, [&](size_t row) {
+        size_t i = row * stride;
         V3 sp = s.p[i], sn = s.n[i];
         uint64_t evals = 0;
         float sum = 0.0f;
@@ -727,9 +729,11 @@ uint64_t build_transfer(const Scene& sc, const Surfels& s, std::vector<Cluster> 
 
 // ------------------------------------------------------------- solve.rs ---
 // solve.rs:27-39
-uint64_t light_surfels(const Scene& sc, Surfels& s, int threads) {
+uint64_t light_surfels(const Scene& sc, Surfels& s, int threads, size_t stride) {
     std::vector<uint64_t> ev(s.size(), 0);
-    parallel_rows(s.size(), threads, [&](size_t i) {
+    if (stride < 1) stride = 1;
+    parallel_rows((s.size() + stride - 1) / stride, threads, [&](size_t row) {
+        size_t i = row * stride;
         uint32_t e;
         V3 c = direct_diffuse(sc, s.p[i], s.n[i], s.albedo[i], e);
         s.direct[i] = c;

@@ -215,15 +215,19 @@ struct Transfer {  // formfactor.rs:48-66
 
 uint32_t normal_bucket(V3 n);                                                 // formfactor.rs:70-89
 void build_clusters(const Scene& sc, const Surfels& s, int32_t res, std::vector<Cluster>& out);  // :91-147
+// stride > 1 computes only rows i with i % stride == 0 (the others stay
+// empty with zero evaluations): a bounded sample of the rows for timing the
+// CPU path at sizes where every row would take too long.
 uint64_t build_transfer(const Scene& sc, const Surfels& s, std::vector<Cluster> clusters, Transfer& t,
-                        int threads);                                         // :153-277
+                        int threads, size_t stride = 1);                      // :153-277
 
 // ---------------------------------------------------------------- solve.rs --
 struct SolveStats {
     uint32_t iterations;
     float residual;
 };
-uint64_t light_surfels(const Scene& sc, Surfels& s, int threads);             // solve.rs:27-39
+// stride as in build_transfer: only surfels i % stride == 0 are lit.
+uint64_t light_surfels(const Scene& sc, Surfels& s, int threads, size_t stride = 1);  // solve.rs:27-39
 // no_exit: run all max_bounces bounces (the residual test never stops the
 // loop), the fixed-K form the gradient is defined on.
 SolveStats solve(Surfels& s, const Transfer& t, uint32_t max_bounces, int threads,

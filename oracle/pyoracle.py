@@ -45,7 +45,8 @@ def lib() -> C.CDLL:
             "orc_surfel_count": (I64, [P]), "orc_get_surfels": (I, [P, P, P, P, P, P, P, P]),
             "orc_set_surfel_state": (I, [P, P, P, P]),
             "orc_build_clusters": (I64, [P, I]), "orc_get_clusters": (I, [P, P, P, P]),
-            "orc_build_transfer": (I, [P, P, P]), "orc_get_transfer": (I, [P, P, P, P, P, P, P, P]),
+            "orc_build_transfer": (I, [P, P, P]), "orc_build_transfer_sampled": (I, [P, I64, P, P]),
+            "orc_light_surfels_sampled": (I64, [P, I64]), "orc_get_transfer": (I, [P, P, P, P, P, P, P, P]),
             "orc_set_transfer": (I, [P, I64, P, I64, P, P]),
             "orc_light_surfels": (I64, [P]), "orc_solve": (I, [P, U32, P, P]),
             "orc_build_grid": (I, [P, P, P]), "orc_get_grid": (I, [P, P, P]), "orc_gather": (I, [P, I64, P, P, P]),
@@ -172,10 +173,12 @@ class Oracle:
         lib().orc_get_clusters(self.h, _p(pnar), _p(off), _p(mem))
         return dict(p=pnar[:, 0:3], n=pnar[:, 3:6], area=pnar[:, 6], radius=pnar[:, 7], offsets=off, members=mem)
 
-    def build_transfer(self) -> dict:
+    def build_transfer(self, stride: int = 1) -> dict:
+        """stride > 1: only rows i % stride == 0 are built (a timing sample);
+        the other rows stay empty."""
         info = np.zeros(4, np.int64)
         mean = np.zeros(1, np.float32)
-        lib().orc_build_transfer(self.h, _p(info), _p(mean))
+        lib().orc_build_transfer_sampled(self.h, stride, _p(info), _p(mean))
         return dict(clusters=int(info[0]), links=int(info[1]), evals=int(info[2]), interior_rows=int(info[3]),
                     mean_row_sum=float(mean[0]))
 
@@ -193,8 +196,9 @@ class Oracle:
         w = f32(w)
         lib().orc_set_transfer(self.h, len(starts) - 1, _p(starts), len(idx), _p(idx), _p(w))
 
-    def light_surfels(self) -> int:
-        return int(lib().orc_light_surfels(self.h))
+    def light_surfels(self, stride: int = 1) -> int:
+        """stride > 1: only surfels i % stride == 0 are lit (a timing sample)."""
+        return int(lib().orc_light_surfels_sampled(self.h, stride))
 
     def solve(self, max_bounces: int, fixed: bool = False):
         """fixed: exactly max_bounces bounces (no residual exit)."""
