@@ -7,7 +7,7 @@
  * crate-internal functions called from src/main.rs. Each entry point below
  * replaces one of those functions; the citation names the reference function
  * (file:line, relative to the crate root) whose behaviour it reproduces. A
- * Rust host binds these with `extern "C"` declarations.
+ * Rust host binds these with an `extern "C"` block that mirrors this header.
  *
  * Conventions
  *  - Every function returns an int status: IFX_OK (0) or an IFX_ERR_* code.
@@ -168,6 +168,17 @@ int ifx_timer_stop(ifx_ctx* ctx, float* ms);
  * scenes are read from global memory through L1. Never changes results.
  * Default 24 KiB, at most 128 KiB. No counterpart in the reference. */
 int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes);
+/* Failure detection: the poll budget of this context's bounded device-side
+ * waits (the scene-staging wait of every ray-marching kernel and the grid
+ * barrier of the one-launch solve). A wait that runs out of polls sets a
+ * status bit, leaves its kernel without tracing (after its own copy in
+ * flight has landed), and the call returns IFX_ERR_TIMEOUT; the context
+ * stays usable. 0 polls makes every such wait give up at once; the default
+ * is IFX_WAIT_LIMIT_DEFAULT. Lowering it is for tests of that error path.
+ * No counterpart in the reference, whose stages cannot fail (it only
+ * validates input, src/scene.rs:106-148). */
+#define IFX_WAIT_LIMIT_DEFAULT (1u << 22)
+int ifx_set_wait_limit(ifx_ctx* ctx, uint32_t polls);
 
 /* Flattens the scene (SDF object program, BVH nodes, planes, lights,
  * materials) into device memory. Must precede every stage below. */
@@ -269,8 +280,13 @@ int ifx_autotune_batched(ifx_ctx* ctx, uint32_t R, const float* E, int* best);
  *   cluster_p_area4  nc  cluster position, w = area (read)
  *   cluster_ranges   nc  [begin, end) of each cluster in `members` (uint2)
  *   members, starts, idx, w   cluster members and the CSR matrix (read)
+ * The float4 arrays must be 16-byte aligned, cluster_ranges 8-byte aligned
+ * and members, starts, idx and w 4-byte aligned; a misaligned pointer is
+ * refused with IFX_ERR_INVALID before anything is launched.
  * `stream` is a cudaStream_t (NULL: the default stream). The call returns
- * after the solve has finished on that stream.
+ * after the solve has finished on that stream. It makes `device` current
+ * for its own work and makes the caller's previous current device current
+ * again before it returns, on every path.
  *
  * The first call on a device looks up the scratch array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call

@@ -28,17 +28,21 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libinterflect_b200.so")
+# IFX_CHECKED=1 selects the bounds-checked build of the same library (test
+# runs only; every scene-array index checked, failures reported as errors).
+LIB_PATH = os.path.join(_HERE, "lib", "libinterflect_b200_checked.so" if os.environ.get("IFX_CHECKED") == "1"
+                        else "libinterflect_b200.so")
 CLI_PATH = os.path.join(_HERE, "bin", "interflect")
 COMPARE_PATH = os.path.join(_HERE, "bin", "compare")
 
 IFX_OK, IFX_ERR_INVALID, IFX_ERR_PARSE, IFX_ERR_CUDA, IFX_ERR_NOMEM, IFX_ERR_LIMIT, IFX_ERR_TIMEOUT = range(7)
+WAIT_LIMIT_DEFAULT = 1 << 22  # IFX_WAIT_LIMIT_DEFAULT
 MODES = {"beauty": 0, "direct": 1, "indirect": 2, "normals": 3, "depth": 4, "steps": 5}
 
 # Every symbol include/interflect.h declares.
 EXPORTS = (
     "ifx_scene_parse", "ifx_scene_free", "ifx_scene_get_info", "ifx_scene_set_cfg", "ifx_scene_set_use_bvh",
-    "ifx_scene_get_bvh",
+    "ifx_scene_get_bvh", "ifx_set_wait_limit",
     "ifx_ctx_create", "ifx_ctx_destroy", "ifx_last_error", "ifx_get_stats", "ifx_scene_upload",
     "ifx_surfels_generate", "ifx_surfels_upload", "ifx_surfels_count", "ifx_surfels_download",
     "ifx_transfer_build", "ifx_transfer_download", "ifx_clusters_download", "ifx_transfer_row_diag",
@@ -67,6 +71,11 @@ class LimitError(ValueError):
 
 class DeviceError(RuntimeError):
     """A CUDA failure, a missing device or a failed device-side check."""
+
+
+class WaitTimeout(DeviceError):
+    """A bounded device-side wait ran out of polls (IFX_ERR_TIMEOUT); the
+    call's results are invalid, the context stays usable."""
 
 
 class _RenderCfg(C.Structure):
@@ -174,6 +183,7 @@ def lib() -> C.CDLL:
         "ifx_multiscene_run": (I, [P, C.POINTER(F)]),
         "ifx_multiscene_download": (I, [P, I, P, P, C.POINTER(_SolveStats)]),
         "ifx_set_stage_limit": (I, [P, U32]),
+        "ifx_set_wait_limit": (I, [P, U32]),
         "ifx_clusters_build": (I, [P, I, C.POINTER(U64)]),
         "ifx_render_reference": (I, [P, C.POINTER(_Camera), U32, U32, U32, F, P, P]),
         "ifx_frame": (I, [P, I, U32, C.POINTER(_Camera), I, U32, U32, F, P, P, C.POINTER(_FrameInfo)]),
@@ -352,6 +362,8 @@ class Context:
             msg = lib().ifx_last_error(self._h).decode(errors="replace")
             if r == IFX_ERR_LIMIT:
                 raise LimitError(f"{what}: {msg}")
+            if r == IFX_ERR_TIMEOUT:
+                raise WaitTimeout(f"{what} failed ({r}): {msg}")
             raise DeviceError(f"{what} failed ({r}): {msg}")
 
     # -- scene / surfels ------------------------------------------------
@@ -600,6 +612,12 @@ class Context:
         fl = C.c_double()
         self._check(lib().ifx_get_work(self._h, KERNELS[kernel], _ptr(counts), C.byref(fl)), "get_work")
         return counts, fl.value
+
+    def set_wait_limit(self, polls: int | None) -> None:
+        """Poll budget of the bounded device-side waits (None: the default);
+        0 makes every wait give up at once, for tests of that error path."""
+        self._check(lib().ifx_set_wait_limit(self._h, WAIT_LIMIT_DEFAULT if polls is None else polls),
+                    "set_wait_limit")
 
     def set_stage_limit(self, max_bytes: int) -> None:
         """Largest geometry program staged in shared memory per CTA (tuning only)."""

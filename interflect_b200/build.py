@@ -2,6 +2,12 @@
 
 Outputs
   interflect_b200/lib/libinterflect_b200.so   CUDA kernels + C ABI (sm_100a)
+  interflect_b200/lib/libinterflect_b200_checked.so
+                                              the same with -DIFX_CHECKED: scene-array
+                                              indices bounds-checked in every kernel and
+                                              the transfer's structures validated, a
+                                              failure reported as an error (tests only;
+                                              selected by IFX_CHECKED=1)
   interflect_b200/bin/interflect              the `interflect render` CLI
   interflect_b200/bin/compare                 the image comparison tool (host only)
 
@@ -10,7 +16,7 @@ root so that every f32 expression rounds exactly as the reference's unfused
 arithmetic does; host code that computes values the device reuses is built
 with -ffp-contract=off for the same reason.
 
-Usage: python -m interflect_b200.build [--force] [--verbose]
+Usage: python -m interflect_b200.build [--force] [--verbose] [--checked]
 """
 from __future__ import annotations
 
@@ -24,6 +30,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "lib", "libinterflect_b200.so")
+LIB_CHECKED = os.path.join(HERE, "lib", "libinterflect_b200_checked.so")
 CLI = os.path.join(HERE, "bin", "interflect")
 COMPARE = os.path.join(HERE, "bin", "compare")
 
@@ -67,28 +74,40 @@ def _run(cmd: list[str], verbose: bool) -> None:
         raise RuntimeError(f"build step failed ({r.returncode}): {' '.join(cmd)}\n{out}")
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
-    os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+def build_library(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    obj_dir = OBJ + ("_checked" if checked else "")
+    lib = LIB_CHECKED if checked else LIB
+    extra = ["-DIFX_CHECKED"] if checked else []
+    os.makedirs(obj_dir, exist_ok=True)
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "interflect.h")]
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJ, src + ".o")
+        o = os.path.join(obj_dir, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs + [__file__]):
-            _run([nvcc(), *ARCH, *NVCC_FLAGS, "-c", s, "-o", o], verbose)
+            _run([nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", s, "-o", o], verbose)
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJ, src + ".o")
+        o = os.path.join(obj_dir, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs + [__file__]):
             _run(["g++", *CXX_FLAGS, "-c", s, "-o", o], verbose)
     cudalib = os.path.join(cuda_root(), "lib64")
-    if force or _stale(LIB, objs):
-        _run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-L", cudalib, "-lcudart_static", "-lpthread", "-ldl",
+    if force or _stale(lib, objs):
+        _run([nvcc(), *ARCH, "-shared", "-o", lib, *objs, "-L", cudalib, "-lcudart_static", "-lpthread", "-ldl",
               "-lrt"], verbose)
+    return lib
+
+
+def build(force: bool = False, verbose: bool = False, checked: bool = True) -> str:
+    """Both library variants, the CLI and the compare tool."""
+    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "interflect.h")]
+    build_library(force, verbose)
+    if checked:
+        build_library(force, verbose, checked=True)
     cli_src = os.path.join(CSRC, "cli.cpp")
     png_src = os.path.join(CSRC, "png.cpp")
     if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, png_src, LIB] + hdrs)):
@@ -101,5 +120,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
-    print(LIB)
+    if "--checked" in sys.argv:
+        print(build_library(force="--force" in sys.argv, verbose="--verbose" in sys.argv, checked=True))
+    else:
+        build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
+        print(LIB)

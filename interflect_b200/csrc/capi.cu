@@ -79,6 +79,9 @@ struct ifx_ctx {
 
     // solve
     DBuf cluster_rad, ctl;
+    DBuf fsolve;  // FusedSolve block of the one-launch solve
+    // poll budget of the bounded device-side waits (staging, grid barrier)
+    uint32_t wait_polls = kDefaultWaitPolls;
     // the transfer in sliced-ELL form for the solve (built with the transfer)
     DBuf sell_len, sell_perm, sell_keys, sell_rows, sell_sizes, sell_off, sell_idx, sell_w;
     bool sell_ready = false;
@@ -106,6 +109,13 @@ struct ifx_ctx {
     // events (fork, join, start and end of its work).
     cudaStream_t st2 = nullptr;
     DBuf shsc;
+    // The transfer's mean row sum (one ordered chain of additions that no
+    // later stage reads) runs on a third stream; ifx_frame joins it just
+    // before the composition. msum: mean (f32 bits), interior row count.
+    cudaStream_t st3 = nullptr;
+    cudaEvent_t mev[2] = {};
+    DBuf msum;
+    bool mean_pending = false;
     cudaEvent_t fev[4] = {};
 
     // lights: current emission per light (float4), for the relight and adjoint
@@ -205,15 +215,23 @@ static void free_buf(DBuf& b) {
     b.cap = 0;
 }
 
+// The error for a non-zero device status word: a bounds check of the
+// checked build (kStatusBounds) or a bounded wait that expired.
+static int status_error(ifx_ctx* ctx, uint32_t s) {
+    if (s & kStatusBounds)
+        return fail(ctx, IFX_ERR_INVALID, "a bounds check failed inside a kernel (status 0x" + std::to_string(s) + ")");
+    return fail(ctx, IFX_ERR_TIMEOUT, "a device-side bounded wait expired (status 0x" + std::to_string(s) + ")");
+}
+
 // Reads and clears the device status word; a set bit means a bounded wait
-// expired inside a kernel.
+// expired inside a kernel (or, in the checked build, a bounds check failed).
 static int check_status(ifx_ctx* ctx) {
     uint32_t s = 0;
     CK(cudaMemcpyAsync(&s, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     if (s) {
         CK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->st));
-        return fail(ctx, IFX_ERR_TIMEOUT, "a device-side bounded wait expired (status 0x" + std::to_string(s) + ")");
+        return status_error(ctx, s);
     }
     return IFX_OK;
 }
@@ -360,6 +378,9 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
     for (int i = 0; i < kShadeEvents; ++i)
         if ((e = cudaEventCreate(&ctx->shev[i])) != cudaSuccess) return bail(e);
     if ((e = cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->st3, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    for (cudaEvent_t& ev : ctx->mev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     for (cudaEvent_t& ev : ctx->fev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreateWithFlags(&ctx->pinned_ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
@@ -370,6 +391,7 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
     if (ensure(ctx, ctx->qcur, 16 * 8) != IFX_OK || ensure(ctx, ctx->qlen, 16) != IFX_OK)
         return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->status, 16) != IFX_OK || ensure(ctx, ctx->small, 64) != IFX_OK ||
+        ensure(ctx, ctx->msum, 16) != IFX_OK ||
         ensure(ctx, ctx->srgb_t, 256 * sizeof(float)) != IFX_OK || ensure(ctx, ctx->ctl, sizeof(SolveCtl)) != IFX_OK)
         return bail(cudaErrorMemoryAllocation);
     if ((e = cudaMemsetAsync(ctx->status.p, 0, 16, ctx->st)) != cudaSuccess) return bail(e);
@@ -397,6 +419,7 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     if (ctx->st2) cudaStreamSynchronize(ctx->st2);
+    if (ctx->st3) cudaStreamSynchronize(ctx->st3);
     DBuf* bufs[] = {&ctx->blob, &ctx->status, &ctx->srgb_t, &ctx->sp, &ctx->sn, &ctx->salb, &ctx->sdir, &ctx->sirr,
                     &ctx->srad, &ctx->keys, &ctx->keys_alt, &ctx->heads, &ctx->head_scan, &ctx->seg_start,
                     &ctx->members, &ctx->cp_tmp, &ctx->cn_tmp, &ctx->valid, &ctx->valid_scan, &ctx->cp, &ctx->cn,
@@ -417,7 +440,7 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w,
                     &ctx->path_sincos, &ctx->shsc, &ctx->lff, &ctx->lvis, &ctx->lq, &ctx->lsc,
                     &ctx->vkey, &ctx->vkey_alt, &ctx->vval, &ctx->vval_alt, &ctx->ckey, &ctx->ckey_alt,
-                    &ctx->cval, &ctx->cval_alt};
+                    &ctx->cval, &ctx->cval_alt, &ctx->fsolve, &ctx->msum};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -427,6 +450,9 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     for (cudaEvent_t ev : ctx->fev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
+    for (cudaEvent_t ev : ctx->mev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->st3) cudaStreamDestroy(ctx->st3);
     if (ctx->st2) cudaStreamDestroy(ctx->st2);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
@@ -526,6 +552,7 @@ extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     ctx->blobref.stage_bytes = reinterpret_cast<const BlobHeader*>(blob.data())->off_lights;
     ctx->blobref.staged = ctx->blobref.stage_bytes <= ctx->stage_limit ? 1 : 0;
     ctx->blobref.stack_depth = maxd + 2;
+    ctx->blobref.wait_polls = ctx->wait_polls;
     ctx->sc = scene_consts(s);
     ctx->has_scene = true;
     ctx->has_transfer = false;
@@ -869,7 +896,9 @@ extern "C" int ifx_clusters_build(ifx_ctx* ctx, int cluster_res, uint64_t* nc) {
     return IFX_OK;
 }
 
-extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out) {
+// defer_mean: leave the mean row sum running on ctx->st3 (ifx_frame joins it
+// and fills out->mean_row_sum and out->interior_rows itself).
+static int transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out, bool defer_mean) {
     if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
     if (cluster_res < 1 || cluster_res > 512) return fail(ctx, IFX_ERR_LIMIT, "cluster resolution must be in 1..512");
     if (ctx->n == 0) return fail(ctx, IFX_ERR_INVALID, "no surfels");
@@ -1005,16 +1034,35 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     // small: [0] mean (f32 bits), [1] interior, [2] evals
     unsigned long long* small = (unsigned long long*)ctx->small.p;
     CK(cudaMemsetAsync(small, 0, 64, ctx->st));
-    launch_mean_row_sum(ctx->st, n, (const uint32_t*)ctx->starts.p, (const float*)ctx->row_sum.p, (float*)&small[0],
-                        &small[1]);
     launch_sum_u64(ctx->st, (const unsigned long long*)ctx->row_evals.p, n, &small[2]);
+    unsigned long long* msum = (unsigned long long*)ctx->msum.p;
+    CK(cudaEventRecord(ctx->mev[0], ctx->st));
+    CK(cudaStreamWaitEvent(ctx->st3, ctx->mev[0], 0));
+    launch_mean_row_sum(ctx->st3, n, (const uint32_t*)ctx->starts.p, (const float*)ctx->row_sum.p, (float*)&msum[0],
+                        &msum[1]);
+    CK(cudaEventRecord(ctx->mev[1], ctx->st3));
     ctx->launches += 2;
     CKL();
+    ctx->mean_pending = true;
     ctx->links = links;
-    if ((r = sell_build(ctx))) return r;
+#ifdef IFX_CHECKED
+    launch_check_transfer(ctx->st, n, nc, links, (const uint32_t*)ctx->starts.p, (const uint32_t*)ctx->idx.p,
+                          (const uint2*)ctx->crange.p, (const uint32_t*)ctx->members.p, status);
+    ctx->launches++;
+#endif
+    if ((r = sell_build(ctx))) {
+        cudaStreamSynchronize(ctx->st3);
+        ctx->mean_pending = false;
+        return r;
+    }
+    if (!defer_mean) CK(cudaStreamWaitEvent(ctx->st, ctx->mev[1], 0));
     CK(cudaEventRecord(ctx->ev1, ctx->st));
-    unsigned long long hs[3];
+    unsigned long long hs[3], hm[2] = {0, 0};
     CK(cudaMemcpyAsync(hs, small, 24, cudaMemcpyDeviceToHost, ctx->st));
+    if (!defer_mean) {
+        CK(cudaMemcpyAsync(hm, msum, 16, cudaMemcpyDeviceToHost, ctx->st));
+        ctx->mean_pending = false;
+    }
     r = check_status(ctx);
     if (r) return r;
     float ms = 0;
@@ -1029,14 +1077,40 @@ extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_in
     frame_changed(ctx);
     if (out) {
         float mean;
-        memcpy(&mean, &hs[0], 4);
+        memcpy(&mean, &hm[0], 4);
         out->clusters = nc;
         out->links = links;
         out->candidates = ncand;
         out->evals = hs[2];
-        out->interior_rows = hs[1];
+        out->interior_rows = hm[1];
         out->mean_row_sum = mean;
     }
+    return IFX_OK;
+}
+
+extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out) {
+    return transfer_build(ctx, cluster_res, out, false);
+}
+
+// Joins a deferred mean row sum in stream order: ctx->st (and whatever later
+// waits on it) runs after it. Its values are read with read_mean.
+static int join_mean(ifx_ctx* ctx) {
+    if (!ctx->mean_pending) return IFX_OK;
+    ctx->mean_pending = false;
+    CK(cudaStreamWaitEvent(ctx->st, ctx->mev[1], 0));
+    return IFX_OK;
+}
+
+// The mean row sum and interior row count of the last transfer build, once
+// ctx->st has joined it.
+static int read_mean(ifx_ctx* ctx, ifx_transfer_info* out) {
+    unsigned long long hm[2];
+    CK(cudaMemcpyAsync(hm, ctx->msum.p, 16, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    float mean;
+    memcpy(&mean, &hm[0], 4);
+    out->mean_row_sum = mean;
+    out->interior_rows = hm[1];
     return IFX_OK;
 }
 
@@ -1188,30 +1262,63 @@ extern "C" int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* ou
         return IFX_OK;
     }
     ENSURE(ctx->cluster_rad, (size_t)ctx->nc * 16);
-    SolveCtl* ctl = (SolveCtl*)ctx->ctl.p;
-    CK(cudaMemsetAsync(ctl, 0, sizeof(SolveCtl), ctx->st));
-    CK(cudaEventRecord(ctx->ev0, ctx->st));
     SolveCtl h{};
-    // Bounces are enqueued in batches; the host looks at the device-side
-    // convergence flag only between batches.
-    const uint32_t kBatch = 16;
-    for (uint32_t it = 0; it < max_bounces;) {
-        uint32_t end = it + kBatch < max_bounces ? it + kBatch : max_bounces;
-        for (; it < end; ++it) {
-            int l = 0;
-            launch_solve_bounce(ctx->st, ctx->sarr(), ctx->n, (const float4*)ctx->cp.p, (const uint2*)ctx->crange.p,
-                                (const uint32_t*)ctx->members.p, ctx->nc, (const uint32_t*)ctx->starts.p,
-                                (const uint32_t*)ctx->idx.p, (const float*)ctx->w.p, (float4*)ctx->cluster_rad.p,
-                                ctl, it, &l, 0, ctx->sell_ready ? &ctx->sellm : nullptr);
-            ctx->launches += (uint64_t)l;
+    const SellMatrix* sell = ctx->sell_ready ? &ctx->sellm : nullptr;
+    // Up to kFusedSolveMaxRows rows the solve is latency-bound (a few
+    // microseconds of work per bounce): all bounces run in one cooperative
+    // launch. Larger systems are bandwidth-bound and take one launch per
+    // phase, where launch overhead is negligible.
+    const int fgrid = ctx->n <= kFusedSolveMaxRows && max_bounces <= kFusedSolveMaxBounces
+                          ? fused_solve_grid(ctx->n, ctx->nc, sell != nullptr)
+                          : 0;
+    if (fgrid > 0) {
+        ENSURE(ctx->fsolve, sizeof(FusedSolve));
+        FusedSolve* fs = (FusedSolve*)ctx->fsolve.p;
+        CK(cudaMemsetAsync(fs, 0, sizeof(FusedSolve), ctx->st));
+        CK(cudaEventRecord(ctx->ev0, ctx->st));
+        if (max_bounces > 0) {
+            if (launch_solve_fused(ctx->st, fgrid, ctx->sarr(), ctx->n, (const float4*)ctx->cp.p,
+                                   (const uint2*)ctx->crange.p, (const uint32_t*)ctx->members.p, ctx->nc,
+                                   (const uint32_t*)ctx->starts.p, (const uint32_t*)ctx->idx.p,
+                                   (const float*)ctx->w.p, sell, (float4*)ctx->cluster_rad.p, fs, max_bounces, 0,
+                                   (uint32_t*)ctx->status.p, ctx->wait_polls) < 0) {
+                cudaGetLastError();
+                return fail(ctx, IFX_ERR_CUDA, "cooperative launch of the solve was refused");
+            }
+            ctx->launches++;
         }
-        CKL();
-        CK(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
-        if (h.done) break;
+        CK(cudaEventRecord(ctx->ev1, ctx->st));
+        uint32_t hv[4];
+        CK(cudaMemcpyAsync(hv, &fs->iterations, 16, cudaMemcpyDeviceToHost, ctx->st));
+        int r = check_status(ctx);
+        if (r) return r;
+        h.iterations = hv[0];
+        h.last_residual = hv[1];
+    } else {
+        SolveCtl* ctl = (SolveCtl*)ctx->ctl.p;
+        CK(cudaMemsetAsync(ctl, 0, sizeof(SolveCtl), ctx->st));
+        CK(cudaEventRecord(ctx->ev0, ctx->st));
+        // Bounces are enqueued in batches; the host looks at the device-side
+        // convergence flag only between batches.
+        const uint32_t kBatch = 16;
+        for (uint32_t it = 0; it < max_bounces;) {
+            uint32_t end = it + kBatch < max_bounces ? it + kBatch : max_bounces;
+            for (; it < end; ++it) {
+                int l = 0;
+                launch_solve_bounce(ctx->st, ctx->sarr(), ctx->n, (const float4*)ctx->cp.p,
+                                    (const uint2*)ctx->crange.p, (const uint32_t*)ctx->members.p, ctx->nc,
+                                    (const uint32_t*)ctx->starts.p, (const uint32_t*)ctx->idx.p,
+                                    (const float*)ctx->w.p, (float4*)ctx->cluster_rad.p, ctl, it, &l, 0, sell);
+                ctx->launches += (uint64_t)l;
+            }
+            CKL();
+            CK(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            if (h.done) break;
+        }
+        CK(cudaEventRecord(ctx->ev1, ctx->st));
+        CK(cudaEventSynchronize(ctx->ev1));
     }
-    CK(cudaEventRecord(ctx->ev1, ctx->st));
-    CK(cudaEventSynchronize(ctx->ev1));
     CK(cudaEventElapsedTime(&ctx->stats.ms_solve, ctx->ev0, ctx->ev1));
     ctx->has_grid = false;
     if (out) {
@@ -1220,6 +1327,15 @@ extern "C" int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* ou
         memcpy(&res, &h.last_residual, 4);
         out->residual = res;
     }
+    return IFX_OK;
+}
+
+static_assert(kDefaultWaitPolls == IFX_WAIT_LIMIT_DEFAULT, "one default poll budget");
+
+extern "C" int ifx_set_wait_limit(ifx_ctx* ctx, uint32_t polls) {
+    if (!ctx) return IFX_ERR_INVALID;
+    ctx->wait_polls = polls;
+    ctx->blobref.wait_polls = ctx->wait_polls;
     return IFX_OK;
 }
 
@@ -1624,20 +1740,29 @@ extern "C" int ifx_frame(ifx_ctx* ctx, int cluster_res, uint32_t max_bounces, co
     CK(cudaStreamWaitEvent(st2, ctx->fev[0], 0));
     CK(cudaMemsetAsync(sc, 0, 17 * 8, st2));
     CK(cudaMemsetAsync(ctx->qlen.p, 0, 16, st2));
+    CK(cudaMemsetAsync(P.status, 0, 4, st2));  // a failed earlier frame may have left it set
     CK(cudaEventRecord(ctx->fev[2], st2));
     ctx->launches += (uint64_t)launch_shade(st2, P, ctx->shev, kShadeFront);
     // Whatever happens on ctx->st from here, the second stream is drained
     // before this call returns.
     auto finish = [&](int code) {
         cudaStreamSynchronize(st2);
+        if (ctx->mean_pending) {
+            cudaStreamSynchronize(ctx->st3);
+            cudaStreamWaitEvent(ctx->st, ctx->mev[1], 0);
+            ctx->mean_pending = false;
+        }
         return code;
     };
     if (cudaGetLastError() != cudaSuccess) return finish(fail(ctx, IFX_ERR_CUDA, "launch failed"));
     if (needs_gi) {
-        if ((r = ifx_transfer_build(ctx, cluster_res, &info.transfer))) return finish(r);
+        // The mean row sum stays on its own stream through the light stage,
+        // the solve and the grid build; it is joined before the composition.
+        if ((r = transfer_build(ctx, cluster_res, &info.transfer, true))) return finish(r);
         if ((r = ifx_light_surfels(ctx, &info.light_evals))) return finish(r);
         if ((r = ifx_solve(ctx, max_bounces, &info.solve))) return finish(r);
         if ((r = ifx_grid_build(ctx, 0.0f))) return finish(r);
+        if ((r = join_mean(ctx))) return finish(r);
         P.grid = ctx->grid;
     }
     // Join: the composition waits for the grid, then ctx->st waits for it.
@@ -1658,7 +1783,7 @@ extern "C" int ifx_frame(ifx_ctx* ctx, int cluster_res, uint32_t max_bounces, co
     if (status) {
         CK(cudaMemsetAsync(P.status, 0, 4, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
-        return fail(ctx, IFX_ERR_TIMEOUT, "a device-side bounded wait expired (status 0x" + std::to_string(status) + ")");
+        return status_error(ctx, status);
     }
     CK(cudaEventElapsedTime(&ctx->stats.ms_shade, ctx->fev[2], ctx->fev[3]));
     float g[7];
@@ -1669,6 +1794,7 @@ extern "C" int ifx_frame(ifx_ctx* ctx, int cluster_res, uint32_t max_bounces, co
     ctx->stats.ms_shadow2 = g[3];
     ctx->stats.ms_shade_other = g[4] + g[5] + g[6];
     CK(cudaEventElapsedTime(&info.ms_frame, ctx->fev[0], ctx->fev[3]));
+    if (needs_gi && (r = read_mean(ctx, &info.transfer))) return r;
     info.shade_evals = e;
     if (out) *out = info;
     return IFX_OK;

@@ -56,6 +56,27 @@ static constexpr float kMaxF = 3.40282347e38f;
 
 // --------------------------------------------------------- scene view -----
 // Views of the program blob (layout.h) in shared or global memory.
+// Device status word bits (written with integer atomicOr, read by the host).
+static constexpr uint32_t kStatusStageTimeout = 1u;
+static constexpr uint32_t kStatusStackOverflow = 2u;
+
+// Index check of the bounds-checked build (-DIFX_CHECKED): an index outside
+// [0, n) sets kStatusBounds and is replaced by 0, so the access stays inside
+// the array and the host reports the failure; in the normal build it is the
+// index itself.
+#ifdef IFX_CHECKED
+__device__ __forceinline__ uint32_t ck_index(uint32_t i, uint32_t n, uint32_t* status) {
+    if (i >= n) {
+        if (status) atomicOr(status, kStatusBounds);
+        return 0u;
+    }
+    return i;
+}
+#define IFX_CK(i, n, status) ::ifx::ck_index((uint32_t)(i), (uint32_t)(n), (status))
+#else
+#define IFX_CK(i, n, status) (i)
+#endif
+
 struct SceneView {
     const DObject* objs;
     const DPrim* prims;
@@ -65,6 +86,8 @@ struct SceneView {
     const DMaterial* mats;
     const uint32_t* linear;
     int n_planes, n_objects, n_nodes, n_lights, n_slights, use_bvh;
+    int n_prims, n_mats;
+    uint32_t* status;  // the kernel's status word (bounds checks of IFX_CHECKED builds)
     // This thread's BVH traversal stack in shared memory: entry i lives at
     // stk[i * stk_stride] (node index) and stkd[i * stk_stride] (the node's
     // box distance, computed when it was pushed); stk_depth entries (the tree
@@ -73,6 +96,17 @@ struct SceneView {
     uint32_t* stk;
     float* stkd;
     int stk_stride, stk_depth;
+
+    // Element access; bounds-checked in IFX_CHECKED builds.
+    __device__ __forceinline__ const DObject& obj(int i) const { return objs[IFX_CK(i, n_planes + n_objects, status)]; }
+    __device__ __forceinline__ const DPrim& prim(int i) const { return prims[IFX_CK(i, n_prims, status)]; }
+    __device__ __forceinline__ const DNode& node(int i) const { return nodes[IFX_CK(i, n_nodes, status)]; }
+    __device__ __forceinline__ const DQuadLight& light(int i) const { return lights[IFX_CK(i, n_lights, status)]; }
+    __device__ __forceinline__ const DSphereLight& slight(int i) const {
+        return slights[IFX_CK(i, n_slights, status)];
+    }
+    __device__ __forceinline__ const DMaterial& mat(uint32_t i) const { return mats[IFX_CK(i, n_mats, status)]; }
+    __device__ __forceinline__ uint32_t lin(int i) const { return linear[IFX_CK(i, n_objects, status)]; }
 };
 
 __device__ __forceinline__ SceneView make_view(const uint8_t* base) {
@@ -95,12 +129,11 @@ __device__ __forceinline__ SceneView make_view(const uint8_t* base) {
     v.n_lights = h->n_lights;
     v.n_slights = h->n_sphere_lights;
     v.use_bvh = h->use_bvh;
+    v.n_prims = h->n_prims;
+    v.n_mats = h->n_materials;
+    v.status = nullptr;
     return v;
 }
-
-// Device status word bits (written with integer atomicOr, read by the host).
-static constexpr uint32_t kStatusStageTimeout = 1u;
-static constexpr uint32_t kStatusStackOverflow = 2u;
 
 // ------------------------------------------------------- work counters ----
 // Tracing functions take a counter policy. NoCount compiles to nothing and is
@@ -151,11 +184,23 @@ struct Counts {
 
 // Copies the program blob into dynamic shared memory with one bulk
 // (non-multicast) async copy completed on an mbarrier, and returns a view of
-// it. The wait is bounded: on expiry the status word gets
-// kStatusStageTimeout and the caller must return without tracing.
-// `bytes` is a multiple of 16 and both addresses are 16-byte aligned.
+// it. The wait is bounded by `polls`: on expiry the status word gets
+// kStatusStageTimeout, the CTA still waits (again bounded, by
+// kStageDrainPolls) for its copy in flight to land so that no copy writes
+// shared memory after the CTA has left, and the caller must return without
+// tracing. `bytes` is a multiple of 16 and both addresses are 16-byte aligned.
+static constexpr uint32_t kStageDrainPolls = 1u << 22;
+__device__ __forceinline__ uint32_t mbar_try_wait(uint32_t bar) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    return done;
+}
 __device__ __forceinline__ bool stage_scene(const uint8_t* gblob, uint32_t bytes, uint8_t* smem,
-                                            uint64_t* mbar, uint32_t* status) {
+                                            uint64_t* mbar, uint32_t* status, uint32_t polls) {
     uint32_t bar = (uint32_t)__cvta_generic_to_shared(mbar);
     uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem);
     if (threadIdx.x == 0) {
@@ -176,15 +221,15 @@ __device__ __forceinline__ bool stage_scene(const uint8_t* gblob, uint32_t bytes
         }
     }
     uint32_t done = 0;
-    for (uint32_t spin = 0; spin < (1u << 22); ++spin) {
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(done)
-            : "r"(bar)
-            : "memory");
+    for (uint32_t spin = 0; spin < polls; ++spin) {
+        done = mbar_try_wait(bar);
         if (done) break;
     }
-    if (!done) atomicOr(status, kStatusStageTimeout);
+    if (!done) {
+        atomicOr(status, kStatusStageTimeout);
+        for (uint32_t spin = 0; spin < kStageDrainPolls; ++spin)
+            if (mbar_try_wait(bar)) break;
+    }
     __syncthreads();
     return __syncthreads_and(done) != 0;
 }
@@ -268,9 +313,9 @@ __device__ __forceinline__ float prim_dist(const DPrim& pr, V p, C& cnt) {
 // sdf.rs:166-172 with the smooth-subtraction extension.
 template <class C>
 __device__ __forceinline__ float obj_dist(const SceneView& sv, const DObject& o, V p, C& cnt) {
-    float d = prim_dist(sv.prims[o.prim], p, cnt);
+    float d = prim_dist(sv.prim(o.prim), p, cnt);
     for (int s = 1; s <= o.nsub; ++s) {
-        float sd = prim_dist(sv.prims[o.prim + s], p, cnt);
+        float sd = prim_dist(sv.prim(o.prim + s), p, cnt);
         cnt.add(o.smooth > 0.0f ? CN_SMOOTH : CN_HARD);
         if (o.smooth > 0.0f) {
             float k = o.smooth;
@@ -304,7 +349,7 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
     cnt.add(CN_SDF);
     DistHit best{kMaxF, 0u};
     for (int i = 0; i < sv.n_planes; ++i) {
-        const DObject o = sv.objs[i];
+        const DObject o = sv.obj(i);
         float d = obj_dist(sv, o, p, cnt);
         if (d < best.d) best = DistHit{d, o.mat};
     }
@@ -320,19 +365,19 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
         const int stride = sv.stk_stride;
         int sp = 0;
         stack[0] = 0;
-        stackd[0] = aabb_dist2(p, sv.nodes[0], cnt);
+        stackd[0] = aabb_dist2(p, sv.node(0), cnt);
         sp = 1;
         bool first = true;
         while (sp > 0) {
             --sp;
             const int ni = (int)stack[sp * stride];
-            const DNode nd = sv.nodes[ni];
+            const DNode nd = sv.node(ni);
             if (!first) cnt.add(CN_NODE);
             first = false;
             if (sq_ge(stackd[sp * stride], best.d)) continue;
             if (nd.count > 0) {
                 for (int k = nd.link; k < nd.link + nd.count; ++k) {
-                    const DObject o = sv.objs[k];
+                    const DObject o = sv.obj(k);
                     float d = obj_dist(sv, o, p, cnt);
                     if (d < best.d) {
                         best.d = d;
@@ -341,8 +386,8 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
                 }
             } else {
                 const int l = ni + 1, r = nd.link;
-                float dl = aabb_dist2(p, sv.nodes[l], cnt);
-                float dr = aabb_dist2(p, sv.nodes[r], cnt);
+                float dl = aabb_dist2(p, sv.node(l), cnt);
+                float dr = aabb_dist2(p, sv.node(r), cnt);
                 // Near-first DFS holds at most depth + 1 entries; the host
                 // sizes the stack to depth + 2 (and rejects trees deeper
                 // than the reference's 64-entry stack). The guard keeps an
@@ -364,7 +409,7 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
         }
     } else {
         for (int k = 0; k < sv.n_objects; ++k) {
-            const DObject o = sv.objs[sv.linear[k]];
+            const DObject o = sv.obj(sv.lin(k));
             float d = obj_dist(sv, o, p, cnt);
             if (d < best.d) {
                 best.d = d;
@@ -383,9 +428,9 @@ __device__ __forceinline__ float scene_dist(const SceneView& sv, V p, C& cnt) {
 // Evaluates leaf `leaf`'s objects into `best` (bvh.rs:118-126).
 template <class C>
 __device__ __forceinline__ void leaf_eval(const SceneView& sv, int leaf, V p, DistHit& best, C& cnt) {
-    const DNode nd = sv.nodes[leaf];
+    const DNode nd = sv.node(leaf);
     for (int k = nd.link; k < nd.link + nd.count; ++k) {
-        const DObject o = sv.objs[k];
+        const DObject o = sv.obj(k);
         const float d = obj_dist(sv, o, p, cnt);
         if (d < best.d) {
             best.d = d;
@@ -404,11 +449,11 @@ __device__ __forceinline__ DistHit dist_mat_warp3(const SceneView& sv, V p, bool
     int next = -1, last = -1;  // leaves still to pop, in order
     float dnext = 0.0f, dlast = 0.0f;
     if (active) {
-        const float d0 = aabb_dist2(p, sv.nodes[0], cnt);
+        const float d0 = aabb_dist2(p, sv.node(0), cnt);
         if (!sq_ge(d0, best.d)) {
-            const int l = 1, r = sv.nodes[0].link;
-            const float dl = aabb_dist2(p, sv.nodes[l], cnt);
-            const float dr = aabb_dist2(p, sv.nodes[r], cnt);
+            const int l = 1, r = sv.node(0).link;
+            const float dl = aabb_dist2(p, sv.node(l), cnt);
+            const float dr = aabb_dist2(p, sv.node(r), cnt);
             if (sq_lt(dl, dr)) {
                 next = l, dnext = dl, last = r, dlast = dr;
             } else {
@@ -453,7 +498,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
     if (active) {
         cnt.add(CN_SDF);
         for (int i = 0; i < sv.n_planes; ++i) {
-            const DObject o = sv.objs[i];
+            const DObject o = sv.obj(i);
             float d = obj_dist(sv, o, p, cnt);
             if (d < best.d) best = DistHit{d, o.mat};
         }
@@ -461,7 +506,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
     if (!sv.use_bvh) {
         if (active) {
             for (int k = 0; k < sv.n_objects; ++k) {
-                const DObject o = sv.objs[sv.linear[k]];
+                const DObject o = sv.obj(sv.lin(k));
                 float d = obj_dist(sv, o, p, cnt);
                 if (d < best.d) {
                     best.d = d;
@@ -480,7 +525,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
     bool first = true;
     if (active) {
         stack[0] = 0;
-        stackd[0] = aabb_dist2(p, sv.nodes[0], cnt);
+        stackd[0] = aabb_dist2(p, sv.node(0), cnt);
         sp = 1;
     }
     int pending = -1;
@@ -488,7 +533,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         while (pending < 0 && sp > 0) {
             --sp;
             const int ni = (int)stack[sp * stride];
-            const DNode nd = sv.nodes[ni];
+            const DNode nd = sv.node(ni);
             // The box distance stored at push time (see dist_mat).
             if (!first) cnt.add(CN_NODE);
             first = false;
@@ -498,8 +543,8 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
                 break;
             }
             const int l = ni + 1, r = nd.link;
-            float dl = aabb_dist2(p, sv.nodes[l], cnt);
-            float dr = aabb_dist2(p, sv.nodes[r], cnt);
+            float dl = aabb_dist2(p, sv.node(l), cnt);
+            float dr = aabb_dist2(p, sv.node(r), cnt);
             if (sp + 2 > sv.stk_depth) {
                 sp = 0;
                 break;
@@ -930,7 +975,7 @@ __device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DM
     V f0{m.f0[0], m.f0[1], m.f0[2]};
     V kd{m.kd[0], m.kd[1], m.kd[2]};
     for (int li = 0; li < sv.n_lights; ++li) {
-        const DQuadLight& L = sv.lights[li];
+        const DQuadLight& L = sv.light(li);
         V lc{L.center[0], L.center[1], L.center[2]};
         V ln{L.normal[0], L.normal[1], L.normal[2]};
         V to_light = lc - p;
@@ -959,7 +1004,7 @@ __device__ __forceinline__ V direct(const SceneView& sv, V p, V n, V v, const DM
         add_specular(out, p, n, v, rep, radius, alpha, n_dot_v, f0, radiance, cnt);
     }
     for (int li = 0; li < sv.n_slights; ++li) {  // extension: sphere lights
-        const DSphereLight& L = sv.slights[li];
+        const DSphereLight& L = sv.slight(li);
         V c{L.c[0], L.c[1], L.c[2]};
         V to_light = c - p;
         float ff = sphere_light_ff(p, n, c, L.c[3]);
@@ -999,7 +1044,7 @@ __device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V alb
     if (terms)
         for (int li = 0; li < sv.n_lights + sv.n_slights; ++li) terms[li] = -1.0f;
     for (int li = 0; li < sv.n_lights; ++li) {
-        const DQuadLight& L = sv.lights[li];
+        const DQuadLight& L = sv.light(li);
         V lc{L.center[0], L.center[1], L.center[2]};
         V ln{L.normal[0], L.normal[1], L.normal[2]};
         V to_light = lc - p;
@@ -1019,7 +1064,7 @@ __device__ __forceinline__ V direct_diffuse(const SceneView& sv, V p, V n, V alb
         if (terms) terms[li] = ff * vis;
     }
     for (int li = 0; li < sv.n_slights; ++li) {  // extension: sphere lights
-        const DSphereLight& L = sv.slights[li];
+        const DSphereLight& L = sv.slight(li);
         V c{L.c[0], L.c[1], L.c[2]};
         V to_light = c - p;
         float ff = sphere_light_ff(p, n, c, L.c[3]);
@@ -1049,7 +1094,7 @@ __device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, flo
     bool found = false;
     float best = 0.0f;
     for (int li = 0; li < sv.n_lights; ++li) {
-        const DQuadLight& L = sv.lights[li];
+        const DQuadLight& L = sv.light(li);
         V nc{L.ncross[0], L.ncross[1], L.ncross[2]};
         float denom = dot(nc, rd);
         if (fabsf(denom) < 1e-9f) continue;
@@ -1069,7 +1114,7 @@ __device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, flo
     }
     if (quads_only) return found;
     for (int li = 0; li < sv.n_slights; ++li) {
-        const DSphereLight& L = sv.slights[li];
+        const DSphereLight& L = sv.slight(li);
         V oc = ro - V{L.c[0], L.c[1], L.c[2]};
         float b = dot(oc, rd);
         float cc = dot(oc, oc) - L.c[3] * L.c[3];
@@ -1089,8 +1134,8 @@ __device__ __forceinline__ bool emitter_hit(const SceneView& sv, V ro, V rd, flo
 
 // Emission of light l (quad lights, then sphere lights).
 __device__ __forceinline__ V light_emit(const SceneView& sv, int l) {
-    if (l < sv.n_lights) return V{sv.lights[l].emit[0], sv.lights[l].emit[1], sv.lights[l].emit[2]};
-    const DSphereLight& S = sv.slights[l - sv.n_lights];
+    if (l < sv.n_lights) return V{sv.light(l).emit[0], sv.light(l).emit[1], sv.light(l).emit[2]};
+    const DSphereLight& S = sv.slight(l - sv.n_lights);
     return V{S.emit[0], S.emit[1], S.emit[2]};
 }
 

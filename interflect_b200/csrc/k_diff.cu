@@ -116,7 +116,7 @@ __device__ __forceinline__ void direct_coeffs(const SceneView& sv, V p, V n, V v
     V f0{m.f0[0], m.f0[1], m.f0[2]};
     V kd{m.kd[0], m.kd[1], m.kd[2]};
     for (int li = 0; li < sv.n_lights; ++li) {
-        const DQuadLight& L = sv.lights[li];
+        const DQuadLight& L = sv.light(li);
         V lc{L.center[0], L.center[1], L.center[2]};
         V ln{L.normal[0], L.normal[1], L.normal[2]};
         if (dot(ln, -nrm(lc - p)) <= 0.0f) continue;
@@ -136,7 +136,7 @@ __device__ __forceinline__ void direct_coeffs(const SceneView& sv, V p, V n, V v
     }
     for (int si = 0; si < sv.n_slights; ++si) {
         const int li = sv.n_lights + si;
-        const DSphereLight& S = sv.slights[si];
+        const DSphereLight& S = sv.slight(si);
         V to_light = V{S.c[0], S.c[1], S.c[2]} - p;
         float ff = ffs[li];
         if (ff <= 1e-6f) continue;
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(128) k_diff_pixels(ShadeParams P, int pass, fl
                          V{P.cam.right[0], P.cam.right[1], P.cam.right[2]} * px +
                          V{P.cam.up[0], P.cam.up[1], P.cam.up[2]} * py);
         const V p = mk4(P.hp1[pix]), n = mk4(b);
-        const DMaterial& m = sv.mats[flags & kPixMatMask];
+        const DMaterial& m = sv.mat(flags & kPixMatMask);
         const V kd{m.kd[0], m.kd[1], m.kd[2]};
         if (pass == 0) direct_coeffs(sv, p, n, -rd, m, P.ff1 + (size_t)pix * nl, P.vis1 + (size_t)pix * nl, one, acc);
         uint32_t count = pass ? gather_entries(g, p, n, kd, put) : gather_entries(g, p, n, kd, nop);
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(128) k_diff_pixels(ShadeParams P, int pass, fl
                 if (pass == 0) acc((int)__float_as_uint(b2.x), fg);
             } else if (f2 & kPixHit) {
                 const V p2 = mk4(a2), n2 = mk4(b2);
-                const DMaterial& m2 = sv.mats[f2 & kPixMatMask];
+                const DMaterial& m2 = sv.mat(f2 & kPixMatMask);
                 if (pass == 0)
                     direct_coeffs(sv, p2, n2, -refl, m2, P.ff2 + (size_t)pix * nl, P.vis2 + (size_t)pix * nl, fg,
                                   acc);

@@ -23,40 +23,7 @@
 
 namespace ifx {
 
-// Bounded grid barrier over the CTAs of one cooperative launch. Returns
-// false (and sets kStatusBarrier in *status) if the other CTAs did not
-// arrive within the poll budget; the caller then leaves the kernel.
-static constexpr uint32_t kStatusBarrier = 1u << 4;
 static constexpr uint32_t kBarrierPolls = 1u << 24;
-
-__device__ __forceinline__ bool grid_barrier(MsBarrier* b, uint32_t* status) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        volatile uint32_t* vgen = &b->gen;
-        const uint32_t g = *vgen;
-        __threadfence();
-        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
-            atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicAdd(&b->gen, 1u);
-        } else {
-            uint32_t polls = 0;
-            while (*vgen == g) {
-                if (++polls > kBarrierPolls) {
-                    atomicOr(status, kStatusBarrier);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(128);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return ok != 0;
-}
 
 // Scene owning packed item `item`: the last scene whose base is <= item.
 __device__ __forceinline__ int scene_of(const uint32_t* base, int S, uint32_t item) {
@@ -93,7 +60,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
         S.rad[i] = f4(out, 0.0f);
         S.irr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
-    if (!grid_barrier(M.bar, M.status)) return;
+    if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
 
     for (uint32_t it = 0; it < M.max_bounces; ++it) {
         // solve.rs:61-73: cluster means, members summed in member order.
@@ -112,7 +79,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
             }
             S.crad[c] = f4(acc / fmaxf(S.cp[c].w, 1e-12f), 0.0f);
         }
-        if (!grid_barrier(M.bar, M.status)) return;
+        if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
         // solve.rs:76-102: Jacobi rows; the residual is the per-scene max.
         for (uint32_t item = tid; item < M.total_surf; item += stride) {
             const int s = scene_of(M.surf_base, M.S, item);
@@ -135,7 +102,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
             bits = __reduce_max_sync(grp, bits);
             if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && bits) atomicMax(&M.ctl[s].residual_bits, bits);
         }
-        if (!grid_barrier(M.bar, M.status)) return;
+        if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
         // solve.rs:454-462 per scene, with each scene's own bounce cap.
         if (blockIdx.x == 0) {
             __shared__ uint32_t live;
@@ -154,7 +121,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
             __syncthreads();
             if (threadIdx.x == 0) M.live[0] = live;
         }
-        if (!grid_barrier(M.bar, M.status)) return;
+        if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
         if (*(volatile uint32_t*)&M.live[0] == 0) break;
     }
 
@@ -164,7 +131,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
         const uint32_t k = item - S.surf_base;
         S.girr[k] = S.irr[S.gitems[k]];
     }
-    if (!grid_barrier(M.bar, M.status)) return;
+    if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
 
     // main.rs:289-358 for every pixel of every scene.
     NoCount cnt;

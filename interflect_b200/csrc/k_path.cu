@@ -137,18 +137,18 @@ __global__ void __launch_bounds__(128) k_path(ShadeParams P, uint32_t spp, const
             }
         }
         if (act == kSurface) {
-            const DMaterial& m = sv.mats[hmat];
+            const DMaterial& m = sv.mat(hmat);
             radiance = radiance + throughput * V{m.emissive[0], m.emissive[1], m.emissive[2]};
             li = 0;
             act = kNee;
         }
         if (act == kNee) {
             // reference.rs:89-118: the next light whose sample needs a shadow ray
-            const DMaterial& m = sv.mats[hmat];
+            const DMaterial& m = sv.mat(hmat);
             const V albedo{m.kd[0], m.kd[1], m.kd[2]};
             act = kBounce;
             for (; li < sv.n_lights; ++li) {
-                const DQuadLight& L = sv.lights[li];
+                const DQuadLight& L = sv.light(li);
                 const V v0{L.v[0][0], L.v[0][1], L.v[0][2]};
                 const V e1 = V{L.v[1][0], L.v[1][1], L.v[1][2]} - v0;
                 const V e2 = V{L.v[3][0], L.v[3][1], L.v[3][2]} - v0;
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(128) k_path(ShadeParams P, uint32_t spp, const
         }
         if (act == kBounce) {
             // reference.rs:120-133
-            const DMaterial& m = sv.mats[hmat];
+            const DMaterial& m = sv.mat(hmat);
             throughput = throughput * V{m.kd[0], m.kd[1], m.kd[2]};
             const V dir = cosine_hemisphere(n, rng, sincos);
             const V origin = hp + n * 1e-3f;

@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(128) k_setup(ShadeParams P) {
                 if (ff > 1e-6f) enqueue(P.q1, &P.qlen[0], slot);
             }
         }
-        if (P.has_gi && sv.mats[flags & kMatMask].f0[3] != 0.0f) enqueue(P.qr, &P.qlen[1], pix);
+        if (P.has_gi && sv.mat(flags & kMatMask).f0[3] != 0.0f) enqueue(P.qr, &P.qlen[1], pix);
     }
     if constexpr (sizeof(C) > 1) cnt.flush(P.counts);
 }
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(128) k_light_compose(ShadeParams P, SurfelArra
             if (f <= 1e-6f) continue;
             const float v = vis[slot];
             if (v <= 1e-4f) continue;
-            const float* e = l < sv.n_lights ? sv.lights[l].emit : sv.slights[l - sv.n_lights].emit;
+            const float* e = l < sv.n_lights ? sv.light(l).emit : sv.slight(l - sv.n_lights).emit;
             out = out + albedo * V{e[0], e[1], e[2]} * (f * v);
             if (terms) terms[slot] = f * v;
         }

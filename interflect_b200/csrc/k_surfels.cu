@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(128) k_gen_finalize(BlobRef blob, const float4
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         V p = mk4(pts[i]);
         DistHit h = dist_mat(sv, p, nc);
-        const DMaterial& m = sv.mats[h.mat];
+        const DMaterial& m = sv.mat(h.mat);
         V nn = scene_normal(sv, p, nc);
         s.p[i] = f4(p, area);
         s.n[i] = f4(nn, 0.0f);

@@ -254,12 +254,15 @@ __global__ void __launch_bounds__(256) k_row_fill(uint32_t n, const unsigned lon
 // row order (the reference's iterator sum starts from -0.0). One CTA: all
 // threads stream chunks of rows into shared memory (rows without links
 // contribute an exact -0.0, the additive identity), thread 0 performs the
-// ordered additions; chunks are double-buffered so loads overlap the adds.
+// ordered additions, four values per 16-byte shared-memory load; chunks are
+// double-buffered so loads overlap the adds. The sum is one dependent chain
+// of additions by nature (f32 addition does not associate), so it runs on
+// its own stream beside the stages that follow it.
 static constexpr int kMeanBlock = 1024;
 __global__ void __launch_bounds__(kMeanBlock) k_mean_row_sum(uint32_t n, const uint32_t* starts,
                                                                const float* row_sum, float* out_mean,
                                                                unsigned long long* out_interior) {
-    __shared__ float buf[2][kMeanBlock];
+    __shared__ __align__(16) float buf[2][kMeanBlock];
     __shared__ unsigned long long cnt;
     if (threadIdx.x == 0) cnt = 0;
     float acc = -0.0f;
@@ -279,8 +282,15 @@ __global__ void __launch_bounds__(kMeanBlock) k_mean_row_sum(uint32_t n, const u
     for (uint32_t c = 0; c < chunks; ++c) {
         const int b = c & 1;
         if (threadIdx.x == 0) {
-#pragma unroll 16
-            for (int k = 0; k < kMeanBlock; ++k) acc += buf[b][k];
+            const float4* b4 = reinterpret_cast<const float4*>(buf[b]);
+#pragma unroll 8
+            for (int k = 0; k < kMeanBlock / 4; ++k) {
+                const float4 v = b4[k];
+                acc += v.x;
+                acc += v.y;
+                acc += v.z;
+                acc += v.w;
+            }
         } else if (c + 1 < chunks) {
             load(c + 1, b ^ 1);
         }
@@ -394,6 +404,31 @@ void launch_mean_row_sum(cudaStream_t st, uint32_t n, const uint32_t* starts, co
 void launch_sum_u64(cudaStream_t st, const unsigned long long* v, uint32_t n, unsigned long long* out) {
     k_sum_u64<<<grid_for(n, 256, 2), 256, 0, st>>>(v, n, out);
 }
+
+#ifdef IFX_CHECKED
+// Bounds-checked build only: every structure the transfer build produced is
+// validated before the solve reads it (CSR starts non-decreasing and ending
+// at `links`, link columns below nc, cluster ranges inside the member list,
+// member indices below n); a violation sets kStatusBounds.
+__global__ void k_check_transfer(uint32_t n, uint32_t nc, unsigned long long links, const uint32_t* starts,
+                                 const uint32_t* idx, const uint2* crange, const uint32_t* members,
+                                 uint32_t* status) {
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long t0 = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool bad = false;
+    for (unsigned long long i = t0; i < n; i += stride) bad |= starts[i] > starts[i + 1] || members[i] >= n;
+    if (t0 == 0) bad |= starts[0] != 0u || starts[n] != links;
+    for (unsigned long long k = t0; k < links; k += stride) bad |= idx[k] >= nc;
+    for (unsigned long long c = t0; c < nc; c += stride) bad |= crange[c].x > crange[c].y || crange[c].y > n;
+    if (bad) atomicOr(status, kStatusBounds);
+}
+void launch_check_transfer(cudaStream_t st, uint32_t n, uint32_t nc, unsigned long long links,
+                           const uint32_t* starts, const uint32_t* idx, const uint2* crange,
+                           const uint32_t* members, uint32_t* status) {
+    k_check_transfer<<<grid_for(links > n ? links : n, 256), 256, 0, st>>>(n, nc, links, starts, idx, crange,
+                                                                          members, status);
+}
+#endif
 
 void configure_transfer_kernels(int max_dyn_smem) {
     cudaFuncSetAttribute(k_visibility<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);

@@ -24,8 +24,9 @@ static inline size_t blob_smem(const BlobRef& b, int block) {
 __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsmem, uint64_t* mbar,
                                                uint32_t* status, SceneView& sv) {
     sv = make_view(blob.ptr);
+    sv.status = status;
     if (blob.staged) {
-        if (!stage_scene(blob.ptr, blob.stage_bytes, dsmem, mbar, status)) return false;
+        if (!stage_scene(blob.ptr, blob.stage_bytes, dsmem, mbar, status, blob.wait_polls)) return false;
         const SceneView s = make_view(dsmem);
         sv.objs = s.objs;
         sv.prims = s.prims;
@@ -44,6 +45,41 @@ __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsm
     __shared__ __align__(8) uint64_t ifx_mbar;                                \
     SceneView sv;                                                             \
     if (!scene_prologue(blob, ifx_dsmem, &ifx_mbar, status, sv)) return;
+
+// Bounded grid barrier over the CTAs of one cooperative launch (every CTA is
+// resident, so all of them arrive unless one has left after an error).
+// Returns false, with kStatusBarrier set in *status, when the other CTAs did
+// not arrive within `polls` polls; the caller then leaves the kernel. The
+// barrier's count must be zero at launch.
+static constexpr uint32_t kStatusBarrier = 1u << 4;
+__device__ __forceinline__ bool grid_barrier(MsBarrier* b, uint32_t* status, uint32_t polls) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile uint32_t* vgen = &b->gen;
+        const uint32_t g = *vgen;
+        __threadfence();
+        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            uint32_t n = 0;
+            while (*vgen == g) {
+                if (++n > polls) {
+                    atomicOr(status, kStatusBarrier);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
 
 // Number of CTAs for a grid-stride kernel: enough to fill every SM several
 // times over, never more than the work needs.

@@ -21,7 +21,13 @@ struct BlobRef {
     uint32_t stage_bytes;
     int staged;
     int stack_depth;  // BVH traversal stack entries per thread (tree depth + 2)
+    uint32_t wait_polls;  // poll budget of the staging wait (kDefaultWaitPolls unless the host lowers it)
 };
+
+// Default poll budget of every bounded device-side wait (the scene-staging
+// mbarrier and the fused solve's grid barrier); the host may lower it per
+// context (ifx_set_wait_limit) so that a test can make a wait run out.
+static constexpr uint32_t kDefaultWaitPolls = 1u << 22;  // IFX_WAIT_LIMIT_DEFAULT
 
 struct CamParams {
     float origin[3], fwd[3], right[3], up[3];
@@ -151,6 +157,17 @@ void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_
 // links stored as [link / 4][lane][link % 4] so that a warp's 32 rows read
 // one contiguous 512-byte block per 4 links. Every row keeps its links in
 // CSR order. perm == nullptr means "use the CSR arrays".
+#ifdef IFX_CHECKED
+// Bounds-checked build: validates the transfer's CSR and cluster structures.
+void launch_check_transfer(cudaStream_t st, uint32_t n, uint32_t nc, unsigned long long links,
+                           const uint32_t* starts, const uint32_t* idx, const uint2* crange,
+                           const uint32_t* members, uint32_t* status);
+#endif
+
+// Bounded grid barrier state of a cooperative launch (kcommon.cuh).
+struct MsBarrier {
+    uint32_t count, gen;
+};
 struct SellMatrix {
     const uint32_t* perm;       // sorted position -> row
     const uint32_t* len;        // sorted position -> link count
@@ -162,6 +179,23 @@ void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const floa
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
                          const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches,
                          int no_exit = 0, const SellMatrix* sell = nullptr);
+// The Jacobi solve in one cooperative launch (k_solve.cu): bounce state in
+// one zeroed block; residual_bits[k] collects bounce k's max change.
+static constexpr int kFusedSolveBlock = 256;
+static constexpr uint32_t kFusedSolveMaxBounces = 256;
+static constexpr uint32_t kFusedSolveMaxRows = 1u << 18;
+struct FusedSolve {
+    MsBarrier bar;
+    uint32_t iterations, last_residual, done, pad;
+    uint32_t residual_bits[kFusedSolveMaxBounces];
+};
+// Grid of the fused solve for n rows and nc clusters (0: cooperative launch
+// unavailable); launch returns 1, or -1 when the launch was refused.
+int fused_solve_grid(uint32_t n, uint32_t nc, bool sell);
+int launch_solve_fused(cudaStream_t st, int grid, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
+                       const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
+                       const float* w, const SellMatrix* sell, float4* cluster_rad, FusedSolve* fs,
+                       uint32_t max_bounces, int no_exit, uint32_t* status, uint32_t polls);
 // Sliced-ELL construction: row link counts (keys) with the identity (vals);
 // after a stable descending sort of (keys, vals), the slice sizes, then the
 // interleaved copy of idx and w.
@@ -305,9 +339,6 @@ struct MsScene {
     uint32_t max_bounces;
     uint32_t surf_base, clus_base, pix_base;  // first packed item of this scene
     ShadeParams P;           // the prepared frame (recompose set)
-};
-struct MsBarrier {
-    uint32_t count, gen;
 };
 struct MsParams {
     const MsScene* scenes;

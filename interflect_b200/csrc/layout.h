@@ -37,6 +37,10 @@ enum PrimKind : int32_t {
 };
 static const int N_PRIM_KINDS = 8;
 
+// Device status bit of the bounds-checked build (IFX_CHECKED): a checked
+// index was out of range.
+static const uint32_t kStatusBounds = 1u << 7;
+
 struct alignas(16) DPrim {
     int32_t kind;
     int32_t pad[3];

@@ -52,6 +52,17 @@ void put_err(char* err, size_t errlen, const char* msg) {
     if (err && errlen) snprintf(err, errlen, "%s", msg);
 }
 
+bool aligned(const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; }
+
+// Puts the caller's current device back when the call returns, whichever
+// way it returns: the entry point selects `device` only for its own work.
+struct DeviceRestore {
+    int prev = -1;
+    ~DeviceRestore() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace
 
 extern "C" int ifx_solve_noalloc(int device, void* stream, uint32_t n, uint32_t nc, const float* p_area4,
@@ -79,7 +90,21 @@ extern "C" int ifx_solve_noalloc(int device, void* stream, uint32_t n, uint32_t 
         put_err(err, errlen, "null device pointer");
         return IFX_ERR_INVALID;
     }
-    cudaError_t e = cudaSetDevice(device);
+    // The kernels read the float4 arrays with 16-byte loads and the cluster
+    // ranges with 8-byte loads; a misaligned pointer (an arena offset aligned
+    // to less) would fault inside a kernel and poison the caller's context,
+    // so it is refused here, before anything is launched.
+    if (!aligned(p_area4, 16) || !aligned(direct4, 16) || !aligned(albedo4, 16) || !aligned(irr4, 16) ||
+        !aligned(rad4, 16) || !aligned(cluster_p_area4, 16) || !aligned(cluster_ranges, 8) ||
+        !aligned(members, 4) || !aligned(starts, 4) || !aligned(idx, 4) || !aligned(w, 4)) {
+        put_err(err, errlen,
+                "misaligned device pointer: float4 arrays need 16-byte, cluster_ranges 8-byte and the index and "
+                "weight arrays 4-byte alignment");
+        return IFX_ERR_INVALID;
+    }
+    DeviceRestore restore;
+    cudaError_t e = cudaGetDevice(&restore.prev);
+    if (e == cudaSuccess) e = cudaSetDevice(device);
     if (e != cudaSuccess) {
         put_err(err, errlen, cudaGetErrorString(e));
         return IFX_ERR_CUDA;

@@ -92,10 +92,10 @@ struct LightGeom {
 };
 __device__ __forceinline__ LightGeom light_geom(const SceneView& sv, int l, V p) {
     if (l < sv.n_lights) {
-        const DQuadLight& L = sv.lights[l];
+        const DQuadLight& L = sv.light(l);
         return LightGeom{V{L.center[0], L.center[1], L.center[2]} - p, L.center[3]};
     }
-    const DSphereLight& S = sv.slights[l - sv.n_lights];
+    const DSphereLight& S = sv.slight(l - sv.n_lights);
     return LightGeom{V{S.c[0], S.c[1], S.c[2]} - p, fmaxf(S.c[3], 1e-4f)};
 }
 
@@ -105,12 +105,12 @@ __device__ __forceinline__ LightGeom light_geom(const SceneView& sv, int l, V p)
 template <class C>
 __device__ __forceinline__ float light_ff(const SceneView& sv, int l, V p, V n, V tan, V bit, C& cnt) {
     if (l < sv.n_lights) {
-        const DQuadLight& L = sv.lights[l];
+        const DQuadLight& L = sv.light(l);
         V to_light = V{L.center[0], L.center[1], L.center[2]} - p;
         if (dot(V{L.normal[0], L.normal[1], L.normal[2]}, -nrm(to_light)) <= 0.0f) return -1.0f;
         return quad_light_ff(L, p, tan, bit, n, cnt);
     }
-    const DSphereLight& S = sv.slights[l - sv.n_lights];
+    const DSphereLight& S = sv.slight(l - sv.n_lights);
     return sphere_light_ff(p, n, V{S.c[0], S.c[1], S.c[2]}, S.c[3]);
 }
 
@@ -125,7 +125,7 @@ __device__ __forceinline__ V direct_from_slots(const SceneView& sv, V p, V n, V 
     V f0{m.f0[0], m.f0[1], m.f0[2]};
     V kd{m.kd[0], m.kd[1], m.kd[2]};
     for (int li = 0; li < sv.n_lights; ++li) {
-        const DQuadLight& L = sv.lights[li];
+        const DQuadLight& L = sv.light(li);
         V lc{L.center[0], L.center[1], L.center[2]};
         V ln{L.normal[0], L.normal[1], L.normal[2]};
         V to_light = lc - p;
@@ -149,7 +149,7 @@ __device__ __forceinline__ V direct_from_slots(const SceneView& sv, V p, V n, V 
     }
     for (int si = 0; si < sv.n_slights; ++si) {
         const int li = sv.n_lights + si;
-        const DSphereLight& S = sv.slights[si];
+        const DSphereLight& S = sv.slight(si);
         V to_light = V{S.c[0], S.c[1], S.c[2]} - p;
         float ff = ffs[li];
         if (ff <= 1e-6f) continue;
@@ -187,7 +187,7 @@ __device__ __forceinline__ void compose_pixel(const SceneView& sv, const ShadePa
     }
     const V rd = camera_ray(P, pix);
     const V p = mk4(P.hp1[pix]), n = mk4(b);
-    const DMaterial& m = sv.mats[flags & kPixMatMask];
+    const DMaterial& m = sv.mat(flags & kPixMatMask);
     V col{0.0f, 0.0f, 0.0f};
     if (P.mode != 2) {
         V d = direct_from_slots(sv, p, n, -rd, m, P.ff1 + (size_t)pix * nl, P.vis1 + (size_t)pix * nl, cnt);
@@ -206,7 +206,7 @@ __device__ __forceinline__ void compose_pixel(const SceneView& sv, const ShadePa
                 rc = light_emit(sv, (int)__float_as_uint(b2.x));
             } else if (f2 & kPixHit) {
                 const V p2 = mk4(a2), n2 = mk4(b2);
-                const DMaterial& m2 = sv.mats[f2 & kPixMatMask];
+                const DMaterial& m2 = sv.mat(f2 & kPixMatMask);
                 V d2 = direct_from_slots(sv, p2, n2, -refl, m2, P.ff2 + (size_t)pix * nl,
                                          P.vis2 + (size_t)pix * nl, cnt);
                 V i2 = gather(g, p2, n2, cnt);

@@ -57,6 +57,7 @@ def test_noalloc_solve_matches_the_context_solve_on_two_calls_in_a_row():
     n, nc = len(s0["area"]), info.clusters
     stream = torch.cuda.current_stream().cuda_stream
 
+    free_after = []
     for call in range(2):
         irr4.zero_()
         rad4.copy_(d4)  # the solve starts from B = E, as after light_surfels
@@ -71,7 +72,30 @@ def test_noalloc_solve_matches_the_context_solve_on_two_calls_in_a_row():
         # Same kernels, same order of operations: bit-identical (tolerance 0).
         assert rad.tobytes() == ref["rad"].tobytes(), call
         assert irr.tobytes() == ref["irr"].tobytes(), call
+        assert torch.cuda.current_device() == 0
+        free_after.append(torch.cuda.mem_get_info(0)[0])
+    # The first call may load the module that holds the static scratch; the
+    # second must leave the device's free memory exactly as it found it (any
+    # cudaMalloc would take at least one 2 MiB granule).
+    assert free_after[1] == free_after[0], free_after
     ctx.close()
+
+
+def test_noalloc_solve_refuses_misaligned_pointers_before_launching():
+    """An arena offset aligned to less than a float4 is refused with an error
+    (no kernel runs, so the caller's context stays usable)."""
+    torch = pytest.importorskip("torch")
+    buf = torch.zeros(1024, dtype=torch.float32, device="cuda:0")
+    base = buf.data_ptr()
+    ptrs = [base + 256 * i for i in range(11)]
+    ptrs[3] += 4  # irr4 on a 4-byte boundary only
+    with pytest.raises(ifx.DeviceError, match="misaligned"):
+        ifx.solve_noalloc(0, 0, 8, 2, *ptrs, 4)
+    ptrs[3] -= 4
+    ptrs[6] += 4  # cluster_ranges on a 4-byte boundary only
+    with pytest.raises(ifx.DeviceError, match="misaligned"):
+        ifx.solve_noalloc(0, 0, 8, 2, *ptrs, 4)
+    torch.cuda.synchronize()  # the context is still healthy
 
 
 def test_noalloc_solve_rejects_more_clusters_than_its_scratch_holds():
