@@ -441,6 +441,11 @@ def run_batch(args, world, rank, local) -> dict | None:
         return None
     value = R * args.steps * world / (t_max / 1e3)
     loop_rate = loop_n / (loop_ms / 1e3)
+    # HBM roofline of the SpMM solve: algorithmic bytes of one step (every
+    # right-hand side's own bounce count) over the step's device time.
+    nbytes = spmm_bytes(info.links, placed, info.clusters, [int(x) for x in its])
+    peak, peak_src = hbm_peak(measured_peaks())
+    gbs = nbytes / (t_max / args.steps / 1e3) / 1e9
     return {
         "metric": BATCH_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -450,7 +455,17 @@ def run_batch(args, world, rank, local) -> dict | None:
                    "bounces_run_max": int(max(its)), "spmm_warps_per_block": tuned,
                    "l2": "flushed (256 MB write) before every timed step"},
         "plain_loop": {"value": loop_rate, "unit": "solves/s", "rhs_timed": loop_n,
-                       "speedup": value / loop_rate},
+                       "speedup": value / loop_rate,
+                       "contains": "per right-hand side: ifx_surfels_set_emission (E uploaded from host memory, "
+                                   "direct = rad = E, irr = 0) then ifx_solve (one cooperative launch, its stop "
+                                   "rule read back by the host), i.e. the single-RHS API a caller would loop over"},
+        "roofline": {"kernel": "k_agg_batched + k_spmm + k_bounce_end_batched", "bound": "hbm", "achieved": gbs,
+                     "peak": peak, "unit": "GB/s", "frac": gbs / peak, "traffic": None,
+                     "bytes_per_step": nbytes, "peak_source": peak_src,
+                     "bytes_model": "per bounce: 8 B/link + 4 B/row start + 20 B/surfel (albedo, area) shared by "
+                                    "all right-hand sides, plus 80 B/surfel + 32 B/cluster per right-hand side "
+                                    "still iterating (E, rad read twice, irr and rad written; cluster values "
+                                    "written and read)"},
         "e2e": {"value": R * args.steps / (e2e_max / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(E.nbytes), "d2h_bytes_per_step": int(2 * E.nbytes)},
         "gpu_launches": int(launches),
@@ -550,7 +565,10 @@ def run_multi(args, world, rank, local) -> dict | None:
                    "pixels_total": sum(m[1].width * m[1].height for m in members),
                    "bounces_run": [int(min(iters)), int(max(iters))], "launch": {"grid": grid, "block": block},
                    "l2": "flushed (256 MB write) before every timed step"},
-        "one_launch_per_scene": {"value": S / (a_max / 1e3), "unit": "scenes/s", "speedup": a_max / t_max},
+        "one_launch_per_scene": {"value": S / (a_max / 1e3), "unit": "scenes/s", "speedup": a_max / t_max,
+                                 "note": "the like-for-like baseline: the same packed kernel launched once per "
+                                         "scene; both re-compose stored hits (geometry, camera and visibility "
+                                         "were traced once at preparation)"},
         "plain_pipeline_loop": {"value": S / (b_max / 1e3), "unit": "scenes/s", "speedup": b_max / t_max,
                                 "note": "ifx_light_surfels + ifx_solve + ifx_grid_build + ifx_render_frame per "
                                         "scene (re-traces every ray)"},
@@ -560,6 +578,21 @@ def run_multi(args, world, rank, local) -> dict | None:
         "gpu_launches": args.steps,
         "clocks": clocks,
     }
+
+
+def spmm_bytes(links: int, n: int, nc: int, its: list[int]) -> int:
+    """Algorithmic bytes of one batched solve: the matrix, row starts, albedo
+    and area once per bounce (the most any right-hand side runs), and per
+    right-hand side per bounce its E, rad (read by the rows and by the
+    cluster means), irr and rad writes and its cluster values."""
+    return (8 * links + 4 * (n + 1) + 20 * n) * max(its) + (80 * n + 32 * nc) * sum(its)
+
+
+def hbm_peak(peaks: dict) -> tuple[float, str]:
+    for k in ("hbm_gbs", "hbm_copy_gbs", "copy_gbs"):
+        if peaks.get(k):
+            return float(peaks[k]), f"MEASURED_PEAKS.json {k} (measured copy bandwidth)"
+    return 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool; MEASURED_PEAKS.json absent)"
 
 
 def solve_bytes(links: int, n: int, nc: int) -> int:

@@ -479,6 +479,53 @@ __device__ __forceinline__ DistHit dist_mat_warp3(const SceneView& sv, V p, bool
     return best;
 }
 
+// dist_mat_warp3's result by another schedule, for the uncounted kernels:
+// each of the two leaves is evaluated at most once per call, by all 32 lanes
+// together (converged), when the box tests say that some lane of the warp
+// may visit it; every lane then replays the reference's own decisions (root
+// pruned? which child first? each leaf pruned against the best so far?).
+// A leaf's effect on the running best is a function of the leaf alone: its
+// objects' sequential strict-`<` updates (bvh.rs:118-126) leave the smaller
+// of the incoming best and the leaf's minimum, with the material of the
+// first object that reaches that minimum. So each leaf is reduced to that
+// pair once, and the replay applies it with the same strict `<`. A lane's
+// result (distance and material) is therefore exactly dist_mat's, while the
+// warp runs no per-leaf rounds.
+__device__ __forceinline__ DistHit leaf_min(const SceneView& sv, const DNode& nd, V p) {
+    NoCount nc;
+    DistHit m{kMaxF, 0u};
+    for (int k = nd.link; k < nd.link + nd.count; ++k) {
+        const DObject o = sv.obj(k);
+        const float d = obj_dist(sv, o, p, nc);
+        if (d < m.d) m = DistHit{d, o.mat};
+    }
+    return m;
+}
+
+__device__ __forceinline__ DistHit dist_mat_warp3_all(const SceneView& sv, V p, bool active, DistHit best) {
+    NoCount nc;
+    const DNode& root = sv.node(0);
+    const DNode& nl = sv.node(1);
+    const DNode& nr = sv.node(root.link);
+    const float d0 = aabb_dist2(p, root, nc);
+    const float dl = aabb_dist2(p, nl, nc);
+    const float dr = aabb_dist2(p, nr, nc);
+    const bool root_in = active && !sq_ge(d0, best.d);
+    // A leaf at or beyond the planes' best is pruned whatever the other leaf gives.
+    const bool may_l = root_in && !sq_ge(dl, best.d);
+    const bool may_r = root_in && !sq_ge(dr, best.d);
+    DistHit ml{kMaxF, 0u}, mr{kMaxF, 0u};
+    if (__any_sync(0xffffffffu, may_l)) ml = leaf_min(sv, nl, p);
+    if (__any_sync(0xffffffffu, may_r)) mr = leaf_min(sv, nr, p);
+    if (!root_in) return best;
+    const bool left_first = sq_lt(dl, dr);
+    const DistHit m1 = left_first ? ml : mr, m2 = left_first ? mr : ml;
+    const float d1 = left_first ? dl : dr, d2 = left_first ? dr : dl;
+    if (!sq_ge(d1, best.d) && m1.d < best.d) best = m1;
+    if (!sq_ge(d2, best.d) && m2.d < best.d) best = m2;
+    return best;
+}
+
 // dist_mat for a whole warp (all 32 lanes call it; lanes with !active only
 // take part in the votes). Each active lane runs its own near-first BVH
 // traversal with the reference's pruning, but leaves are evaluated in
@@ -517,7 +564,12 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         return best;
     }
     if (sv.n_nodes == 0) return best;
-    if (sv.n_nodes == 3) return dist_mat_warp3(sv, p, active, best, cnt);
+    if (sv.n_nodes == 3) {
+        // The counting kernels keep the reference's schedule (their counts
+        // are the algorithmic work); the others replay its decisions.
+        if constexpr (sizeof(C) == 1) return dist_mat_warp3_all(sv, p, active, best);
+        return dist_mat_warp3(sv, p, active, best, cnt);
+    }
     uint32_t* const stack = sv.stk;
     float* const stackd = sv.stkd;
     const int stride = sv.stk_stride;
@@ -795,6 +847,23 @@ __device__ __forceinline__ V scene_normal_rolled(const SceneView& sv, V p, C& cn
     for (int i = 0; i < 4; ++i) {
         V k{(i == 0 || i == 3) ? 1.0f : -1.0f, (i >= 2) ? 1.0f : -1.0f, (i == 1 || i == 3) ? 1.0f : -1.0f};
         n = n + k * scene_dist(sv, p + k * H, cnt);
+    }
+    float l = len(n);
+    if (l > 1e-12f) return n / l;
+    return V{0.0f, 1.0f, 0.0f};
+}
+
+// scene_normal_rolled for a whole warp: the same four taps and arithmetic,
+// each tap a warp-collective dist_mat_warp query (all 32 lanes call this;
+// lanes with !active only take part in the votes and their result is unused).
+template <class C>
+__device__ __forceinline__ V scene_normal_w(const SceneView& sv, V p, bool active, C& cnt) {
+    const float H = 5e-4f;
+    V n{0.0f, 0.0f, 0.0f};
+#pragma unroll 1
+    for (int i = 0; i < 4; ++i) {
+        V k{(i == 0 || i == 3) ? 1.0f : -1.0f, (i >= 2) ? 1.0f : -1.0f, (i == 1 || i == 3) ? 1.0f : -1.0f};
+        n = n + k * dist_mat_warp(sv, p + k * H, active, cnt).d;
     }
     float l = len(n);
     if (l > 1e-12f) return n / l;
