@@ -38,7 +38,7 @@ CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "k_ba
               "k_path.cu", "capi.cu", "noalloc.cu"]
 CPP_SOURCES = ["scene_host.cpp"]
 HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh", "shade.cuh", "flop_model.h",
-           "sqcmp.h", "pixorder.h"]
+           "sqcmp.h", "pixorder.h", "libm_f32.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "layout.h"
+#include "libm_f32.h"
 #include "sqcmp.h"
 
 namespace ifx {
@@ -479,53 +480,6 @@ __device__ __forceinline__ DistHit dist_mat_warp3(const SceneView& sv, V p, bool
     return best;
 }
 
-// dist_mat_warp3's result by another schedule, for the uncounted kernels:
-// each of the two leaves is evaluated at most once per call, by all 32 lanes
-// together (converged), when the box tests say that some lane of the warp
-// may visit it; every lane then replays the reference's own decisions (root
-// pruned? which child first? each leaf pruned against the best so far?).
-// A leaf's effect on the running best is a function of the leaf alone: its
-// objects' sequential strict-`<` updates (bvh.rs:118-126) leave the smaller
-// of the incoming best and the leaf's minimum, with the material of the
-// first object that reaches that minimum. So each leaf is reduced to that
-// pair once, and the replay applies it with the same strict `<`. A lane's
-// result (distance and material) is therefore exactly dist_mat's, while the
-// warp runs no per-leaf rounds.
-__device__ __forceinline__ DistHit leaf_min(const SceneView& sv, const DNode& nd, V p) {
-    NoCount nc;
-    DistHit m{kMaxF, 0u};
-    for (int k = nd.link; k < nd.link + nd.count; ++k) {
-        const DObject o = sv.obj(k);
-        const float d = obj_dist(sv, o, p, nc);
-        if (d < m.d) m = DistHit{d, o.mat};
-    }
-    return m;
-}
-
-__device__ __forceinline__ DistHit dist_mat_warp3_all(const SceneView& sv, V p, bool active, DistHit best) {
-    NoCount nc;
-    const DNode& root = sv.node(0);
-    const DNode& nl = sv.node(1);
-    const DNode& nr = sv.node(root.link);
-    const float d0 = aabb_dist2(p, root, nc);
-    const float dl = aabb_dist2(p, nl, nc);
-    const float dr = aabb_dist2(p, nr, nc);
-    const bool root_in = active && !sq_ge(d0, best.d);
-    // A leaf at or beyond the planes' best is pruned whatever the other leaf gives.
-    const bool may_l = root_in && !sq_ge(dl, best.d);
-    const bool may_r = root_in && !sq_ge(dr, best.d);
-    DistHit ml{kMaxF, 0u}, mr{kMaxF, 0u};
-    if (__any_sync(0xffffffffu, may_l)) ml = leaf_min(sv, nl, p);
-    if (__any_sync(0xffffffffu, may_r)) mr = leaf_min(sv, nr, p);
-    if (!root_in) return best;
-    const bool left_first = sq_lt(dl, dr);
-    const DistHit m1 = left_first ? ml : mr, m2 = left_first ? mr : ml;
-    const float d1 = left_first ? dl : dr, d2 = left_first ? dr : dl;
-    if (!sq_ge(d1, best.d) && m1.d < best.d) best = m1;
-    if (!sq_ge(d2, best.d) && m2.d < best.d) best = m2;
-    return best;
-}
-
 // dist_mat for a whole warp (all 32 lanes call it; lanes with !active only
 // take part in the votes). Each active lane runs its own near-first BVH
 // traversal with the reference's pruning, but leaves are evaluated in
@@ -564,12 +518,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         return best;
     }
     if (sv.n_nodes == 0) return best;
-    if (sv.n_nodes == 3) {
-        // The counting kernels keep the reference's schedule (their counts
-        // are the algorithmic work); the others replay its decisions.
-        if constexpr (sizeof(C) == 1) return dist_mat_warp3_all(sv, p, active, best);
-        return dist_mat_warp3(sv, p, active, best, cnt);
-    }
+    if (sv.n_nodes == 3) return dist_mat_warp3(sv, p, active, best, cnt);
     uint32_t* const stack = sv.stk;
     float* const stackd = sv.stkd;
     const int stride = sv.stk_stride;
@@ -853,23 +802,6 @@ __device__ __forceinline__ V scene_normal_rolled(const SceneView& sv, V p, C& cn
     return V{0.0f, 1.0f, 0.0f};
 }
 
-// scene_normal_rolled for a whole warp: the same four taps and arithmetic,
-// each tap a warp-collective dist_mat_warp query (all 32 lanes call this;
-// lanes with !active only take part in the votes and their result is unused).
-template <class C>
-__device__ __forceinline__ V scene_normal_w(const SceneView& sv, V p, bool active, C& cnt) {
-    const float H = 5e-4f;
-    V n{0.0f, 0.0f, 0.0f};
-#pragma unroll 1
-    for (int i = 0; i < 4; ++i) {
-        V k{(i == 0 || i == 3) ? 1.0f : -1.0f, (i >= 2) ? 1.0f : -1.0f, (i == 1 || i == 3) ? 1.0f : -1.0f};
-        n = n + k * dist_mat_warp(sv, p + k * H, active, cnt).d;
-    }
-    float l = len(n);
-    if (l > 1e-12f) return n / l;
-    return V{0.0f, 1.0f, 0.0f};
-}
-
 // ltc.rs:88-96
 __device__ __forceinline__ void frame(V n, V& t, V& b) {
     float s = n.z >= 0.0f ? 1.0f : -1.0f;
@@ -880,42 +812,6 @@ __device__ __forceinline__ void frame(V n, V& t, V& b) {
 }
 
 // -------------------------------------------------------------- ltc.rs ----
-// acos in f32 by the published fdlibm method (Sun Microsystems, 1993,
-// e_acosf): pi/2 - (x + x*R(x^2)) for |x| < 1/2 and 2*asin(sqrt((1-x)/2))
-// beyond, with R a degree-(6,4) rational approximation and pi/2 split into
-// high and low parts. It is the algorithm of glibc's acosf, which the
-// reference calls through Rust's f32::acos on Linux; evaluated with IEEE f32
-// operations and no FMA it returns glibc's result for every input in
-// [-1, 1] (checked over all 2,130,706,434 of them).
-__device__ __forceinline__ float acos_f32(float x) {
-    const float pi = __uint_as_float(0x40490fdau), pio2_hi = __uint_as_float(0x3fc90fdau),
-                pio2_lo = __uint_as_float(0x33a22168u);
-    const float p0 = __uint_as_float(0x3e2aaaabu), p1 = __uint_as_float(0xbea6b090u),
-                p2 = __uint_as_float(0x3e4e0aa8u), p3 = __uint_as_float(0xbd241146u),
-                p4 = __uint_as_float(0x3a4f7f04u), p5 = __uint_as_float(0x3811ef08u);
-    const float q1 = __uint_as_float(0xc019d139u), q2 = __uint_as_float(0x4001572du),
-                q3 = __uint_as_float(0xbf303361u), q4 = __uint_as_float(0x3d9dc62eu);
-    const uint32_t hx = __float_as_uint(x), ix = hx & 0x7fffffffu;
-    if (ix == 0x3f800000u) return (hx >> 31) ? pi + 2.0f * pio2_lo : 0.0f;
-    if (ix > 0x3f800000u) return (x - x) / (x - x);
-    float z;
-    if (ix < 0x3f000000u) {
-        if (ix <= 0x32800000u) return pio2_hi + pio2_lo;
-        z = x * x;
-    } else {
-        z = ((hx >> 31) ? (1.0f + x) : (1.0f - x)) * 0.5f;
-    }
-    const float p = z * (p0 + z * (p1 + z * (p2 + z * (p3 + z * (p4 + z * p5)))));
-    const float q = 1.0f + z * (q1 + z * (q2 + z * (q3 + z * q4)));
-    const float r = p / q;
-    if (ix < 0x3f000000u) return pio2_hi - (x - (pio2_lo - x * r));
-    const float s = sqrtf(z);
-    if (hx >> 31) return pi - 2.0f * (s + (r * s - pio2_lo));
-    const float df = __uint_as_float(__float_as_uint(s) & 0xfffff000u);
-    const float c = (z - df * df) / (s + df);
-    return 2.0f * (df + (r * s + c));
-}
-
 // ltc.rs:25-83 on a quad already in the local frame.
 template <class C>
 __device__ __forceinline__ float quad_form_factor(const V l[4], C& cnt) {
@@ -966,7 +862,10 @@ __device__ __forceinline__ float quad_light_ff(const DQuadLight& L, V p, V t, V 
 }
 
 // Extension: horizon-clipped sphere-light form factor (Snyder 1996 closed
-// form, as written by Lagarde & de Rousiers 2014).
+// form, as written by Lagarde & de Rousiers 2014). Its acos and atan are
+// libm_f32.h's, equal to glibc's acosf/atanf, which the oracle calls: the
+// horizon branch subtracts nearly equal terms, so an atan that differed by
+// an ulp would show as a relative difference of up to 1e-3 in the result.
 __device__ __forceinline__ float sphere_light_ff(V p, V n, V c, float r) {
     V d = c - p;
     float dist2 = dot(d, d);
@@ -980,7 +879,7 @@ __device__ __forceinline__ float sphere_light_ff(V p, V n, V c, float r) {
     float sin_t = sqrtf(fmaxf(1.0f - cos_t * cos_t, 0.0f));
     float y = clampr(-x * (cos_t / sin_t), -1.0f, 1.0f);
     float sty = sin_t * sqrtf(1.0f - y * y);
-    float ill = (cos_t * acos_f32(y) - x * sty) * sin_s2 + atanf(sty / x);
+    float ill = (cos_t * acos_f32(y) - x * sty) * sin_s2 + atan_f32(sty / x);
     return fmaxf(ill, 0.0f) * (1.0f / kPiF);
 }
 

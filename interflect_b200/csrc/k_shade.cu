@@ -81,45 +81,41 @@ __global__ void __launch_bounds__(128) k_setup(ShadeParams P) {
     const uint32_t total = P.w * P.h;
     const V org{P.cam.origin[0], P.cam.origin[1], P.cam.origin[2]};
     const bool tonemapped = P.mode <= 2;
-    // Warp-uniform loop (blockDim is a multiple of 32): the normal's taps are
-    // warp-collective queries.
-    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
-        const uint32_t t = base + threadIdx.x;
-        bool need_n = false;
-        uint32_t pix = 0, flags = 0;
-        float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b = a;
-        if (t < total) {
-            pix = tile_pixel(t, P.w, P.h);  // the queues then fill in tile order
-            a = P.hp1[pix];
-            b = P.hn1[pix];
-            flags = __float_as_uint(b.w);
-            const bool hit = (flags & kFlagHit) != 0;
-            const V rd = camera_ray(P, pix);
-            V e;
-            int which = 0;
-            if (emitter_hit(sv, org, rd, fminf(hit ? a.w : kMaxF, P.tmax), e, &which)) {
-                write_pixel(P, t8, pix, tonemapped ? e : V{0.9f, 0.9f, 0.9f});
-                // The light's index stays with the pixel for re-composition.
-                P.hn1[pix] = make_float4(b.x, __uint_as_float((uint32_t)which), 0.0f,
-                                         __uint_as_float(flags | kFlagDone | kFlagEmit));
-            } else if (!hit) {
-                write_pixel(P, t8, pix, sky());
-                P.hn1[pix].w = __uint_as_float(flags | kFlagDone);
-            } else if (P.mode == 4) {  // depth
-                float d = 1.0f - clampr(a.w / P.tmax, 0.0f, 1.0f);
-                write_pixel(P, t8, pix, V{d * d, d * d, d * d});
-                P.hn1[pix].w = __uint_as_float(flags | kFlagDone);
-            } else if (P.mode == 5) {  // steps
-                float f = (float)__float_as_uint(b.x) / 128.0f;
-                write_pixel(P, t8, pix, V{f, 1.0f - f, 0.2f});
-                P.hn1[pix].w = __uint_as_float(flags | kFlagDone);
-            } else {
-                need_n = true;
-            }
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t pix = tile_pixel(t, P.w, P.h);  // the queues then fill in tile order
+        const float4 a = P.hp1[pix];
+        const float4 b = P.hn1[pix];
+        const uint32_t flags = __float_as_uint(b.w);
+        const bool hit = (flags & kFlagHit) != 0;
+        const V rd = camera_ray(P, pix);
+        V e;
+        int which = 0;
+        if (emitter_hit(sv, org, rd, fminf(hit ? a.w : kMaxF, P.tmax), e, &which)) {
+            write_pixel(P, t8, pix, tonemapped ? e : V{0.9f, 0.9f, 0.9f});
+            // The light's index stays with the pixel for re-composition.
+            P.hn1[pix] = make_float4(b.x, __uint_as_float((uint32_t)which), 0.0f,
+                                     __uint_as_float(flags | kFlagDone | kFlagEmit));
+            continue;
+        }
+        if (!hit) {
+            write_pixel(P, t8, pix, sky());
+            P.hn1[pix].w = __uint_as_float(flags | kFlagDone);
+            continue;
+        }
+        if (P.mode == 4) {  // depth
+            float d = 1.0f - clampr(a.w / P.tmax, 0.0f, 1.0f);
+            write_pixel(P, t8, pix, V{d * d, d * d, d * d});
+            P.hn1[pix].w = __uint_as_float(flags | kFlagDone);
+            continue;
+        }
+        if (P.mode == 5) {  // steps
+            float f = (float)__float_as_uint(b.x) / 128.0f;
+            write_pixel(P, t8, pix, V{f, 1.0f - f, 0.2f});
+            P.hn1[pix].w = __uint_as_float(flags | kFlagDone);
+            continue;
         }
         const V p = mk4(a);
-        const V n = scene_normal_w(sv, p, need_n, cnt);
-        if (!need_n) continue;
+        const V n = scene_normal_rolled(sv, p, cnt);
         if (P.mode == 3) {  // normals
             write_pixel(P, t8, pix, n * 0.5f + V{0.5f, 0.5f, 0.5f});
             P.hn1[pix].w = __uint_as_float(flags | kFlagDone);
@@ -231,32 +227,24 @@ __global__ void __launch_bounds__(128) k_setup2(ShadeParams P) {
     IFX_SCENE_PROLOGUE(P.blob, P.status, sv);
     C cnt;
     const uint32_t total = P.qlen[1];
-    // Warp-uniform loop: the normal's taps are warp-collective queries.
-    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
-        const uint32_t j = base + threadIdx.x;
-        bool need_n = false;
-        uint32_t pix = 0, flags = 0;
-        float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (j < total) {
-            pix = P.qr[j];
-            const V rd = camera_ray(P, pix);
-            const V p = mk4(P.hp1[pix]), n = mk4(P.hn1[pix]);
-            const V refl = rd - n * (2.0f * dot(n, rd));
-            a = P.hp2[pix];
-            flags = __float_as_uint(P.hn2[pix].w);
-            const bool hit = (flags & kFlagHit) != 0;
-            V e;
-            int which = 0;
-            if (emitter_hit(sv, p, refl, fminf(hit ? a.w : kMaxF, P.tmax), e, &which)) {
-                P.hn2[pix] = make_float4(__uint_as_float((uint32_t)which), 0.0f, 0.0f,
-                                         __uint_as_float(flags | kFlagEmit));
-            } else if (hit) {
-                need_n = true;
-            }
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+        const uint32_t pix = P.qr[j];
+        const V rd = camera_ray(P, pix);
+        const V p = mk4(P.hp1[pix]), n = mk4(P.hn1[pix]);
+        const V refl = rd - n * (2.0f * dot(n, rd));
+        const float4 a = P.hp2[pix];
+        const uint32_t flags = __float_as_uint(P.hn2[pix].w);
+        const bool hit = (flags & kFlagHit) != 0;
+        V e;
+        int which = 0;
+        if (emitter_hit(sv, p, refl, fminf(hit ? a.w : kMaxF, P.tmax), e, &which)) {
+            P.hn2[pix] = make_float4(__uint_as_float((uint32_t)which), 0.0f, 0.0f,
+                                     __uint_as_float(flags | kFlagEmit));
+            continue;
         }
+        if (!hit) continue;
         const V p2 = mk4(a);
-        const V n2 = scene_normal_w(sv, p2, need_n, cnt);
-        if (!need_n) continue;
+        const V n2 = scene_normal_rolled(sv, p2, cnt);
         P.hn2[pix] = f4(n2, __uint_as_float(flags));
         V tan, bit;
         frame(n2, tan, bit);

@@ -77,7 +77,17 @@ __device__ __forceinline__ void cluster_mean(const float4* rad, const float4* sp
         const int b = ch & 1;
         if (threadIdx.x == 0) {
             const uint32_t cnt = min((uint32_t)kBlock, len - ch * kBlock);
-            for (uint32_t k = 0; k < cnt; ++k) {
+            // Unrolled so that the shared-memory loads run ahead of the
+            // chain of additions (which stays in member order).
+            uint32_t k = 0;
+            for (; k + 8 <= cnt; k += 8) {
+                float4 v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) v[j] = buf[b][k + j];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc = acc + V{v[j].x, v[j].y, v[j].z};
+            }
+            for (; k < cnt; ++k) {
                 float4 v = buf[b][k];
                 acc = acc + V{v.x, v.y, v.z};
             }
@@ -314,7 +324,9 @@ int fused_solve_grid(uint32_t n, uint32_t nc, bool sell) {
     if (ps <= 0) return 0;
     const unsigned long long need_rows = ((unsigned long long)n + kFusedSolveBlock - 1) / kFusedSolveBlock;
     unsigned long long need = need_rows > nc ? need_rows : nc;
-    const unsigned long long cap = (unsigned long long)ps * (unsigned long long)sm_count();
+    // At most one CTA per SM: the grid barrier's cost grows with the number
+    // of CTAs arriving; rows and clusters are taken grid-stride.
+    const unsigned long long cap = (unsigned long long)sm_count();
     if (need < 1) need = 1;
     return (int)(need < cap ? need : cap);
 }

@@ -165,8 +165,13 @@ void launch_check_transfer(cudaStream_t st, uint32_t n, uint32_t nc, unsigned lo
 #endif
 
 // Bounded grid barrier state of a cooperative launch (kcommon.cuh).
-struct MsBarrier {
-    uint32_t count, gen;
+// The arrival count and the generation word sit on separate 128-byte lines,
+// so that the CTAs polling `gen` do not contend with the arrivals' atomics.
+struct alignas(128) MsBarrier {
+    uint32_t count;
+    uint32_t pad0[31];
+    uint32_t gen;
+    uint32_t pad1[31];
 };
 struct SellMatrix {
     const uint32_t* perm;       // sorted position -> row
