@@ -178,6 +178,12 @@ int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes);
  * No counterpart in the reference, whose stages cannot fail (it only
  * validates input, src/scene.rs:106-148). */
 #define IFX_WAIT_LIMIT_DEFAULT (1u << 22)
+/* Tuning: whether the next ifx_scene_upload builds the per-cell candidate
+ * leaf lists that the cone-shadow marches of large BVHs (more than three
+ * nodes, no cones) use in place of a full traversal, falling back to the
+ * traversal of src/bvh.rs:100-150 whenever the two could differ. Never
+ * changes results. Default on. No counterpart in the reference. */
+int ifx_set_leaf_grid(ifx_ctx* ctx, int on);
 int ifx_set_wait_limit(ifx_ctx* ctx, uint32_t polls);
 
 /* Flattens the scene (SDF object program, BVH nodes, planes, lights,

@@ -42,7 +42,7 @@ MODES = {"beauty": 0, "direct": 1, "indirect": 2, "normals": 3, "depth": 4, "ste
 # Every symbol include/interflect.h declares.
 EXPORTS = (
     "ifx_scene_parse", "ifx_scene_free", "ifx_scene_get_info", "ifx_scene_set_cfg", "ifx_scene_set_use_bvh",
-    "ifx_scene_get_bvh", "ifx_set_wait_limit",
+    "ifx_scene_get_bvh", "ifx_set_wait_limit", "ifx_set_leaf_grid",
     "ifx_ctx_create", "ifx_ctx_destroy", "ifx_last_error", "ifx_get_stats", "ifx_scene_upload",
     "ifx_surfels_generate", "ifx_surfels_upload", "ifx_surfels_count", "ifx_surfels_download",
     "ifx_transfer_build", "ifx_transfer_download", "ifx_clusters_download", "ifx_transfer_row_diag",
@@ -184,6 +184,7 @@ def lib() -> C.CDLL:
         "ifx_multiscene_download": (I, [P, I, P, P, C.POINTER(_SolveStats)]),
         "ifx_set_stage_limit": (I, [P, U32]),
         "ifx_set_wait_limit": (I, [P, U32]),
+        "ifx_set_leaf_grid": (I, [P, I]),
         "ifx_clusters_build": (I, [P, I, C.POINTER(U64)]),
         "ifx_render_reference": (I, [P, C.POINTER(_Camera), U32, U32, U32, F, P, P]),
         "ifx_frame": (I, [P, I, U32, C.POINTER(_Camera), I, U32, U32, F, P, P, C.POINTER(_FrameInfo)]),
@@ -618,6 +619,11 @@ class Context:
         0 makes every wait give up at once, for tests of that error path."""
         self._check(lib().ifx_set_wait_limit(self._h, WAIT_LIMIT_DEFAULT if polls is None else polls),
                     "set_wait_limit")
+
+    def set_leaf_grid(self, on: bool) -> None:
+        """Whether the next upload builds the per-cell leaf lists of large
+        BVHs for cone-shadow marches (results are identical either way)."""
+        self._check(lib().ifx_set_leaf_grid(self._h, 1 if on else 0), "set_leaf_grid")
 
     def set_stage_limit(self, max_bytes: int) -> None:
         """Largest geometry program staged in shared memory per CTA (tuning only)."""

@@ -35,7 +35,7 @@ CLI = os.path.join(HERE, "bin", "interflect")
 COMPARE = os.path.join(HERE, "bin", "compare")
 
 CU_SOURCES = ["k_surfels.cu", "k_transfer.cu", "k_solve.cu", "k_shade.cu", "k_batch.cu", "k_diff.cu", "k_multi.cu",
-              "k_path.cu", "capi.cu", "noalloc.cu"]
+              "k_path.cu", "k_leafgrid.cu", "capi.cu", "noalloc.cu"]
 CPP_SOURCES = ["scene_host.cpp"]
 HEADERS = ["layout.h", "scene_host.h", "kernels.h", "device.cuh", "kcommon.cuh", "shade.cuh", "flop_model.h",
            "sqcmp.h", "pixorder.h", "libm_f32.h"]

@@ -55,6 +55,10 @@ struct ifx_ctx {
     DBuf blob;
     BlobRef blobref{};
     uint32_t stage_limit = kDefaultStageLimit;
+    bool scene_bvh = false;  // the uploaded program traverses a BVH
+    bool leafgrid_on = true;  // build per-cell leaf lists for large BVHs (ifx_set_leaf_grid)
+    DBuf lg_U, lg_count, lg_start, lg_leaves, lg_leaf, lg_key;
+    uint32_t lg_cells = 0, lg_entries = 0;
     SceneConsts sc{};
     DBuf status;  // uint32 device status word
     DBuf srgb_t;  // 256 f32 thresholds
@@ -143,6 +147,7 @@ struct ifx_ctx {
     // scratch
     DBuf cub_tmp, small;  // small: 8 x u64 counters / results
     DBuf gen_cand, gen_keep, gen_off, gen_head, gen_pts, gen_next, gen_state, gen_out;  // surfel generation
+    DBuf gen_head_acc, gen_next_acc;
 
     // measurement: per-kernel events, work counters (IFX_NUM_KERNELS x 21 u64), timer
     cudaEvent_t kv0 = nullptr, kv1 = nullptr, kc0 = nullptr, kc1 = nullptr, tm0 = nullptr, tm1 = nullptr;
@@ -440,7 +445,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w,
                     &ctx->path_sincos, &ctx->shsc, &ctx->lff, &ctx->lvis, &ctx->lq, &ctx->lsc,
                     &ctx->vkey, &ctx->vkey_alt, &ctx->vval, &ctx->vval_alt, &ctx->ckey, &ctx->ckey_alt,
-                    &ctx->cval, &ctx->cval_alt, &ctx->fsolve, &ctx->msum};
+                    &ctx->cval, &ctx->cval_alt, &ctx->fsolve, &ctx->msum, &ctx->gen_head_acc, &ctx->gen_next_acc, &ctx->lg_U, &ctx->lg_count,
+                    &ctx->lg_start, &ctx->lg_leaves, &ctx->lg_leaf, &ctx->lg_key};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (cudaEvent_t ev : {ctx->ev0, ctx->ev1, ctx->kv0, ctx->kv1, ctx->kc0, ctx->kc1, ctx->tm0, ctx->tm1})
@@ -509,11 +515,102 @@ extern "C" int ifx_timer_stop(ifx_ctx* ctx, float* ms) {
     return IFX_OK;
 }
 
+// Staging of the scene program for the ray-marching kernels: the whole
+// geometry prefix when it fits the limit, else (BVH scenes) the header,
+// objects and BVH nodes alone when those fit, else nothing (read through L1).
+static void choose_staging(ifx_ctx* ctx) {
+    BlobRef& b = ctx->blobref;
+    if (b.stage_bytes <= ctx->stage_limit) b.staged = 1;
+    else if (ctx->scene_bvh && b.part_nodes > 0 && align16(b.part_head) + b.part_nodes <= ctx->stage_limit)
+        b.staged = 2;
+    else b.staged = 0;
+}
+
 extern "C" int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes) {
     if (!ctx) return IFX_ERR_INVALID;
     if (max_bytes > kMaxStageLimit) return fail(ctx, IFX_ERR_LIMIT, "stage limit above 128 KiB");
     ctx->stage_limit = max_bytes;
-    if (ctx->has_scene) ctx->blobref.staged = ctx->blobref.stage_bytes <= max_bytes ? 1 : 0;
+    if (ctx->has_scene) choose_staging(ctx);
+    return IFX_OK;
+}
+
+// The leaf grid of a scene with a BVH of more than three nodes whose objects
+// all have exact distance functions (every kind but the cone): 64 cells along
+// the longest side of the scene bounds.
+static int leafgrid_build(ifx_ctx* ctx, const std::vector<uint8_t>& blob) {
+    ctx->blobref.lg = LeafGrid{};
+    const BlobHeader* bh = reinterpret_cast<const BlobHeader*>(blob.data());
+    if (!ctx->leafgrid_on || !bh->use_bvh || bh->n_nodes <= 3) return IFX_OK;
+    const DPrim* prims = reinterpret_cast<const DPrim*>(blob.data() + bh->off_prims);
+    for (int i = 0; i < bh->n_prims; ++i)
+        if (prims[i].kind == K_CONE) return IFX_OK;
+    const DNode* nodes = reinterpret_cast<const DNode*>(blob.data() + bh->off_nodes);
+    std::vector<uint32_t> leaves;
+    for (int i = 0; i < bh->n_nodes; ++i)
+        if (nodes[i].count > 0) leaves.push_back((uint32_t)i);
+    const float* lo = ctx->sc.lo;
+    const float* hi = ctx->sc.hi;
+    double ext = 0.0, mag = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        ext = std::max(ext, (double)hi[a] - (double)lo[a]);
+        mag = std::max(mag, std::max(std::fabs((double)lo[a]), std::fabs((double)hi[a])));
+    }
+    if (!(ext > 0.0)) return IFX_OK;
+    const int kCells = 64;
+    const double cs = ext / kCells;
+    LeafGrid g{};
+    uint32_t ncells = 1;
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = lo[a];
+        g.dim[a] = std::min(kCells, std::max(1, (int)std::ceil(((double)hi[a] - (double)lo[a]) / cs)));
+        ncells *= (uint32_t)g.dim[a];
+    }
+    g.inv_cell = (float)(1.0 / cs);
+    // 2^-12 of the coordinates' scale: thousands of times any f32 rounding
+    // of a distance at that scale, small against the distances marched.
+    g.tol = (float)((mag + (double)ctx->sc.diag) / 4096.0);
+    const double pad = g.tol;
+    const float half_diag = (float)((cs * 0.5 + pad) * std::sqrt(3.0) * (1.0 + 1e-6) + pad);
+    const uint32_t nleaf = (uint32_t)leaves.size();
+    ENSURE(ctx->lg_U, (size_t)ncells * 4);
+    ENSURE(ctx->lg_count, ((size_t)ncells + 1) * 4);
+    ENSURE(ctx->lg_start, ((size_t)ncells + 1) * 4);
+    ENSURE(ctx->lg_leaves, (size_t)nleaf * 4);
+    CK(cudaMemcpyAsync(ctx->lg_leaves.p, leaves.data(), (size_t)nleaf * 4, cudaMemcpyHostToDevice, ctx->st));
+    float* U = (float*)ctx->lg_U.p;
+    uint32_t* count = (uint32_t*)ctx->lg_count.p;
+    uint32_t* start = (uint32_t*)ctx->lg_start.p;
+    launch_lg_bound(ctx->st, ctx->blobref, g, (float)cs, half_diag, ncells, U, (uint32_t*)ctx->status.p);
+    launch_lg_lists(ctx->st, (const uint8_t*)ctx->blob.p, g, cs, pad, ncells, U, (const uint32_t*)ctx->lg_leaves.p,
+                    nleaf, count, nullptr, nullptr, nullptr);
+    CK(cudaMemsetAsync(count + ncells, 0, 4, ctx->st));
+    ctx->launches += 2;
+    CKL();
+    CUB([&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, count, start, (int)ncells + 1, ctx->st);
+    });
+    uint32_t total = 0;
+    CK(cudaMemcpyAsync(&total, start + ncells, 4, cudaMemcpyDeviceToHost, ctx->st));
+    int r = check_status(ctx);  // synchronises
+    if (r) return r;
+    ENSURE(ctx->lg_leaf, (size_t)total * 4);
+    ENSURE(ctx->lg_key, (size_t)total * 4);
+    launch_lg_lists(ctx->st, (const uint8_t*)ctx->blob.p, g, cs, pad, ncells, U, (const uint32_t*)ctx->lg_leaves.p,
+                    nleaf, nullptr, start, (uint32_t*)ctx->lg_leaf.p, (float*)ctx->lg_key.p);
+    ctx->launches++;
+    CKL();
+    g.start = start;
+    g.leaf = (const uint32_t*)ctx->lg_leaf.p;
+    g.enabled = 1;
+    ctx->blobref.lg = g;
+    ctx->lg_entries = total;
+    ctx->lg_cells = ncells;
+    return IFX_OK;
+}
+
+extern "C" int ifx_set_leaf_grid(ifx_ctx* ctx, int on) {
+    if (!ctx) return IFX_ERR_INVALID;
+    ctx->leafgrid_on = on != 0;
     return IFX_OK;
 }
 
@@ -550,10 +647,25 @@ extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     ctx->blobref.ptr = (const uint8_t*)ctx->blob.p;
     ctx->blobref.bytes = (uint32_t)blob.size();
     ctx->blobref.stage_bytes = reinterpret_cast<const BlobHeader*>(blob.data())->off_lights;
-    ctx->blobref.staged = ctx->blobref.stage_bytes <= ctx->stage_limit ? 1 : 0;
+    {
+        const BlobHeader* bh = reinterpret_cast<const BlobHeader*>(blob.data());
+        ctx->blobref.part_head = bh->off_prims;
+        ctx->blobref.part_nodes_off = bh->off_nodes;
+        ctx->blobref.part_nodes = (uint32_t)bh->n_nodes * (uint32_t)sizeof(DNode);
+        ctx->scene_bvh = bh->use_bvh != 0;
+    }
+    choose_staging(ctx);
     ctx->blobref.stack_depth = maxd + 2;
     ctx->blobref.wait_polls = ctx->wait_polls;
+    {
+        const BlobHeader* bh = reinterpret_cast<const BlobHeader*>(blob.data());
+        ctx->blobref.tree3 = bh->use_bvh && bh->n_nodes == 3 ? 1 : 0;
+    }
     ctx->sc = scene_consts(s);
+    {
+        int r = leafgrid_build(ctx, blob);
+        if (r) return r;
+    }
     ctx->has_scene = true;
     ctx->has_transfer = false;
     ctx->has_grid = false;
@@ -680,11 +792,14 @@ extern "C" int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* pla
     ENSURE(ctx->gen_keep, ((size_t)kChunk + 1) * 4);
     ENSURE(ctx->gen_off, ((size_t)kChunk + 1) * 4);
     ENSURE(ctx->gen_head, ncells * 4);
+    ENSURE(ctx->gen_head_acc, ncells * 4);
+    ENSURE(ctx->gen_next_acc, (size_t)seeds * 4);
     ENSURE(ctx->gen_pts, (size_t)seeds * sizeof(float4));
     ENSURE(ctx->gen_next, (size_t)seeds * 4);
     ENSURE(ctx->gen_state, (size_t)seeds * 4);
     ENSURE(ctx->gen_out, (size_t)target * sizeof(float4));
     CK(cudaMemsetAsync(ctx->gen_head.p, 0, ncells * 4, ctx->st));
+    CK(cudaMemsetAsync(ctx->gen_head_acc.p, 0, ncells * 4, ctx->st));
     GenGrid g{};
     for (int a = 0; a < 3; ++a) {
         g.lo[a] = lo[a];
@@ -694,6 +809,8 @@ extern "C" int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* pla
     g.d_min_sq = d_min_sq;
     g.head = (uint32_t*)ctx->gen_head.p;
     g.next = (uint32_t*)ctx->gen_next.p;
+    g.head_acc = (uint32_t*)ctx->gen_head_acc.p;
+    g.next_acc = (uint32_t*)ctx->gen_next_acc.p;
     g.pts = (float4*)ctx->gen_pts.p;
     g.state = (uint32_t*)ctx->gen_state.p;
     g.cap = seeds;
@@ -739,6 +856,7 @@ extern "C" int ifx_surfels_generate(ifx_ctx* ctx, uint64_t target, uint64_t* pla
         const uint32_t quota = (uint32_t)(target - placed_n);
         ctx->launches += (uint64_t)launch_gen_emit(ctx->st, g, base, kept, off, quota,
                                                    (float4*)ctx->gen_out.p + placed_n);
+        ctx->launches += (uint64_t)launch_gen_retire(ctx->st, g, base, kept);
         CKL();
         if ((r = check_status(ctx))) return r;
         placed_n += acc_n < quota ? acc_n : quota;

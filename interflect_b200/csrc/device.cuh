@@ -89,6 +89,7 @@ struct SceneView {
     int n_planes, n_objects, n_nodes, n_lights, n_slights, use_bvh;
     int n_prims, n_mats;
     uint32_t* status;  // the kernel's status word (bounds checks of IFX_CHECKED builds)
+    LeafGrid lg;       // per-cell candidate leaves (shadow marches in large BVHs)
     // This thread's BVH traversal stack in shared memory: entry i lives at
     // stk[i * stk_stride] (node index) and stkd[i * stk_stride] (the node's
     // box distance, computed when it was pushed); stk_depth entries (the tree
@@ -133,6 +134,7 @@ __device__ __forceinline__ SceneView make_view(const uint8_t* base) {
     v.n_prims = h->n_prims;
     v.n_mats = h->n_materials;
     v.status = nullptr;
+    v.lg = LeafGrid{};
     return v;
 }
 
@@ -159,11 +161,21 @@ enum CounterId : int {
     kNumCounters = 21
 };
 
+//
+// kTree3: the scene's BVH is known (by the host, which picks the kernel) to
+// be a root with two leaves, so the distance queries compile only that
+// traversal; a kernel then carries a fraction of the code, which matters to
+// instruction-fetch-bound ray marches. NoCount3 is NoCount for such scenes.
 struct NoCount {
+    static constexpr bool kTree3 = false;
     __device__ __forceinline__ void add(int, uint32_t = 1) {}
+};
+struct NoCount3 : NoCount {
+    static constexpr bool kTree3 = true;
 };
 
 struct Counts {
+    static constexpr bool kTree3 = false;
     uint32_t v[kNumCounters];
     __device__ __forceinline__ Counts() {
 #pragma unroll
@@ -190,6 +202,8 @@ struct Counts {
 // kStageDrainPolls) for its copy in flight to land so that no copy writes
 // shared memory after the CTA has left, and the caller must return without
 // tracing. `bytes` is a multiple of 16 and both addresses are 16-byte aligned.
+// A second range (bytes2 > 0: gsrc2 to smem + off2, the same rules) can ride
+// on the same mbarrier.
 static constexpr uint32_t kStageDrainPolls = 1u << 22;
 __device__ __forceinline__ uint32_t mbar_try_wait(uint32_t bar) {
     uint32_t done;
@@ -200,8 +214,20 @@ __device__ __forceinline__ uint32_t mbar_try_wait(uint32_t bar) {
         : "memory");
     return done;
 }
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const uint8_t* src, uint32_t bytes, uint32_t bar) {
+    const uint32_t kChunk = 32768u;
+    for (uint32_t off = 0; off < bytes; off += kChunk) {
+        uint32_t n = bytes - off < kChunk ? bytes - off : kChunk;
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst + off),
+            "l"(src + off), "r"(n), "r"(bar)
+            : "memory");
+    }
+}
 __device__ __forceinline__ bool stage_scene(const uint8_t* gblob, uint32_t bytes, uint8_t* smem,
-                                            uint64_t* mbar, uint32_t* status, uint32_t polls) {
+                                            uint64_t* mbar, uint32_t* status, uint32_t polls,
+                                            const uint8_t* gsrc2 = nullptr, uint32_t bytes2 = 0,
+                                            uint32_t off2 = 0) {
     uint32_t bar = (uint32_t)__cvta_generic_to_shared(mbar);
     uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem);
     if (threadIdx.x == 0) {
@@ -210,16 +236,10 @@ __device__ __forceinline__ bool stage_scene(const uint8_t* gblob, uint32_t bytes
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-        const uint32_t kChunk = 32768u;
-        for (uint32_t off = 0; off < bytes; off += kChunk) {
-            uint32_t n = bytes - off < kChunk ? bytes - off : kChunk;
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    dst + off),
-                "l"(gblob + off), "r"(n), "r"(bar)
-                : "memory");
-        }
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes + bytes2)
+                     : "memory");
+        bulk_copy(dst, gblob, bytes, bar);
+        if (bytes2) bulk_copy(dst + off2, gsrc2, bytes2, bar);
     }
     uint32_t done = 0;
     for (uint32_t spin = 0; spin < polls; ++spin) {
@@ -353,6 +373,29 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
         const DObject o = sv.obj(i);
         float d = obj_dist(sv, o, p, cnt);
         if (d < best.d) best = DistHit{d, o.mat};
+    }
+    if constexpr (C::kTree3) {
+        // bvh.rs:100-150 on a root and two leaves: the same tests, prunes and
+        // visit order as the stack traversal below.
+        if (sq_ge(aabb_dist2(p, sv.node(0), cnt), best.d)) return best;
+        const int r = sv.node(0).link;
+        const float dl = aabb_dist2(p, sv.node(1), cnt), dr = aabb_dist2(p, sv.node(r), cnt);
+        const bool lfirst = sq_lt(dl, dr);
+#pragma unroll 1
+        for (int pass = 0; pass < 2; ++pass) {
+            const bool left = (pass == 0) == lfirst;
+            if (sq_ge(left ? dl : dr, best.d)) continue;
+            const DNode& nd = sv.node(left ? 1 : r);
+            for (int k = nd.link; k < nd.link + nd.count; ++k) {
+                const DObject o = sv.obj(k);
+                const float d = obj_dist(sv, o, p, cnt);
+                if (d < best.d) {
+                    best.d = d;
+                    best.mat = o.mat;
+                }
+            }
+        }
+        return best;
     }
     if (sv.use_bvh) {
         if (sv.n_nodes == 0) return best;
@@ -504,6 +547,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
             if (d < best.d) best = DistHit{d, o.mat};
         }
     }
+    if constexpr (C::kTree3) return dist_mat_warp3(sv, p, active, best, cnt);
     if (!sv.use_bvh) {
         if (active) {
             for (int k = 0; k < sv.n_objects; ++k) {
@@ -734,11 +778,93 @@ __device__ __forceinline__ int trace_step(const SceneView& sv, TraceRay& r, V& p
     return kMarching;
 }
 
+// Scene::dist (scene.rs:211-213) for a cone-shadow step, through the cell's
+// candidate leaves instead of the BVH: the planes, then each listed leaf whose
+// box is nearer than best + tol, its objects' minimum taken with the same
+// strict `<`. Returns that minimum G; `ok` says whether G is exactly the value
+// the reference's pruned near-first query (bvh.rs:100-150) returns:
+//  * a leaf not listed, or listed but skipped, lies at least best + tol away,
+//    and every object's distance is at least its leaf box's distance less a
+//    rounding error far below tol (exact SDFs; measured below 3e-7 on the
+//    stress scene), so no object outside the evaluated leaves is below G;
+//  * the reference evaluates every plane, and reaches the leaf L1 holding G
+//    unless it prunes L1 or an ancestor, which needs a best <= box(L1) first;
+//    so G is its answer when G is a plane's, when box(L1) <= G, or when no
+//    other leaf or plane reaches box(L1) (then nothing can have pruned L1).
+// Otherwise (and outside the grid) ok is false and the caller asks the
+// reference query.
+__device__ __forceinline__ float dist_fast(const SceneView& sv, V p, bool& ok) {
+    NoCount nc;
+    const LeafGrid& g = sv.lg;
+    float P = kMaxF;
+    for (int i = 0; i < sv.n_planes; ++i) {
+        const float d = obj_dist(sv, sv.obj(i), p, nc);
+        if (d < P) P = d;
+    }
+    ok = false;
+    const float fx = (p.x - g.lo[0]) * g.inv_cell, fy = (p.y - g.lo[1]) * g.inv_cell,
+                fz = (p.z - g.lo[2]) * g.inv_cell;
+    if (!(fx >= 0.0f && fy >= 0.0f && fz >= 0.0f && fx < (float)g.dim[0] && fy < (float)g.dim[1] &&
+          fz < (float)g.dim[2]))
+        return P;
+    const uint32_t cell = (uint32_t)fx + (uint32_t)g.dim[0] * ((uint32_t)fy + (uint32_t)g.dim[1] * (uint32_t)fz);
+    const uint32_t e = __ldg(&g.start[cell + 1]);
+    float best = P, m1 = kMaxF, m2 = kMaxF, d2_1 = 0.0f;
+    for (uint32_t k = __ldg(&g.start[cell]); k < e; ++k) {
+        const DNode& nd = sv.node((int)__ldg(&g.leaf[k]));
+        const float d2 = aabb_dist2(p, nd, nc);
+        const float lim = best + g.tol;
+        if (!(lim > 0.0f) || d2 >= lim * lim) continue;
+        float m = kMaxF;
+        for (int j = nd.link; j < nd.link + nd.count; ++j) {
+            const float d = obj_dist(sv, sv.obj(j), p, nc);
+            if (d < m) m = d;
+        }
+        if (m < m1) {
+            m2 = m1;
+            m1 = m;
+            d2_1 = d2;
+        } else if (m < m2) {
+            m2 = m;
+        }
+        if (m < best) best = m;
+    }
+    if (P <= m1) {
+        ok = true;
+        return P;
+    }
+    const float v1 = sqrtf(d2_1);
+    ok = v1 <= m1 || (m2 > v1 && P > v1);
+    return m1;
+}
+
+// The distance a cone-shadow step needs, for a whole warp: dist_fast where
+// the scene has a leaf grid (uncounted kernels), the reference query for the
+// lanes it cannot answer exactly, dist_mat_warp everywhere else.
+template <class C>
+__device__ __forceinline__ float shadow_dist_w(const SceneView& sv, V p, bool active, C& cnt) {
+    if constexpr (sizeof(C) == 1 && !C::kTree3) {
+        if (sv.lg.enabled) {
+            bool ok = true;
+            float h = 0.0f;
+            if (active) h = dist_fast(sv, p, ok);
+            const bool need = active && !ok;
+            if (__any_sync(0xffffffffu, need)) {
+                const float r = dist_mat_warp(sv, p, need, cnt).d;
+                if (need) h = r;
+            }
+            return h;
+        }
+    }
+    return dist_mat_warp(sv, p, active, cnt).d;
+}
+
 // Warp-collective forms of the two steps above: all 32 lanes call them, the
-// SDF query is dist_mat_warp, and lanes with !active change nothing.
+// SDF query is dist_mat_warp (shadow_dist_w for the cone march), and lanes
+// with !active change nothing.
 template <class C>
 __device__ __forceinline__ bool shadow_step_w(const SceneView& sv, ShadowRay& s, bool active, float& vis, C& cnt) {
-    const float h = dist_mat_warp(sv, s.ro + s.rd * s.t, active, cnt).d;
+    const float h = shadow_dist_w(sv, s.ro + s.rd * s.t, active, cnt);
     if (!active) return false;
     cnt.add(CN_SSTEP);
     s.steps += 1;
@@ -783,6 +909,25 @@ __device__ __forceinline__ int trace_step_w(const SceneView& sv, TraceRay& r, bo
         return kHit;
     }
     r.t += h.d;
+    if (r.t > r.tmax || r.steps >= kMaxSteps) return kMiss;
+    return kMarching;
+}
+
+// trace_step_w for marches that need only hit or miss and the step count
+// (the hemisphere closure, trace.rs:165-186): the query is shadow_dist_w's,
+// whose value is the reference's exactly, so the march is the same.
+template <class C>
+__device__ __forceinline__ int trace_step_dist_w(const SceneView& sv, TraceRay& r, bool active, C& cnt) {
+    const float hd = shadow_dist_w(sv, r.ro + r.rd * r.t, active, cnt);
+    if (!active) return kMarching;
+    cnt.add(CN_TSTEP);
+    r.steps += 1;
+    float eps = 1e-4f * fmaxf(r.t, 1.0f);
+    if (hd < eps) {
+        r.steps += 4;
+        return kHit;
+    }
+    r.t += hd;
     if (r.t > r.tmax || r.steps >= kMaxSteps) return kMiss;
     return kMarching;
 }

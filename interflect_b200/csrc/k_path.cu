@@ -216,6 +216,8 @@ int launch_path(cudaStream_t st, const ShadeParams& p, uint32_t spp, const float
     const unsigned long long px = (unsigned long long)p.w * p.h;
     if (p.counts)
         k_path<Counts><<<persistent_grid(k_path<Counts>, 128, sm, px), 128, sm, st>>>(p, spp, sincos, cursor);
+    else if (p.blob.tree3)
+        k_path<NoCount3><<<persistent_grid(k_path<NoCount3>, 128, sm, px), 128, sm, st>>>(p, spp, sincos, cursor);
     else
         k_path<NoCount><<<persistent_grid(k_path<NoCount>, 128, sm, px), 128, sm, st>>>(p, spp, sincos, cursor);
     return 1;
@@ -223,6 +225,7 @@ int launch_path(cudaStream_t st, const ShadeParams& p, uint32_t spp, const float
 
 void configure_path_kernels(int max_dyn_smem) {
     cudaFuncSetAttribute(k_path<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_path<NoCount3>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
     cudaFuncSetAttribute(k_path<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }
 

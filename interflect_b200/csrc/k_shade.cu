@@ -324,6 +324,7 @@ static void launch_all(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev, i
 
 int launch_shade(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev, int part) {
     if (p.counts) launch_all<Counts>(st, p, ev, part);
+    else if (p.blob.tree3) launch_all<NoCount3>(st, p, ev, part);
     else launch_all<NoCount>(st, p, ev, part);
     return ((part & kShadeFront) ? (p.has_gi ? 6 : 3) : 0) + ((part & kShadeCompose) ? 1 : 0);
 }
@@ -390,6 +391,10 @@ int launch_light_slots(cudaStream_t st, const ShadeParams& p, const SurfelArrays
         k_light_setup<Counts><<<grid_for(n, 128, 16), 128, sm, st>>>(p, s.p, s.n, n, ff);
         k_shadow<Counts><<<persistent_grid(k_shadow<Counts>, 128, sm, slots), 128, sm, st>>>(
             p, s.p, s.n, p.q1, &p.qlen[0], vis, cursor);
+    } else if (p.blob.tree3) {
+        k_light_setup<NoCount3><<<grid_for(n, 128, 16), 128, sm, st>>>(p, s.p, s.n, n, ff);
+        k_shadow<NoCount3><<<persistent_grid(k_shadow<NoCount3>, 128, sm, slots), 128, sm, st>>>(
+            p, s.p, s.n, p.q1, &p.qlen[0], vis, cursor);
     } else {
         k_light_setup<NoCount><<<grid_for(n, 128, 16), 128, sm, st>>>(p, s.p, s.n, n, ff);
         k_shadow<NoCount><<<persistent_grid(k_shadow<NoCount>, 128, sm, slots), 128, sm, st>>>(
@@ -403,7 +408,10 @@ int launch_compose(cudaStream_t st, const ShadeParams& p) {
     const size_t sm = blob_smem(p.blob, 128);
     ShadeParams q = p;
     q.counts = nullptr;
-    k_compose<NoCount><<<grid_for((unsigned long long)p.w * p.h, 128, 16), 128, sm, st>>>(q);
+    if (p.blob.tree3)
+        k_compose<NoCount3><<<grid_for((unsigned long long)p.w * p.h, 128, 16), 128, sm, st>>>(q);
+    else
+        k_compose<NoCount><<<grid_for((unsigned long long)p.w * p.h, 128, 16), 128, sm, st>>>(q);
     return 1;
 }
 
@@ -419,8 +427,10 @@ static void configure_one(int max_dyn_smem) {
 
 void configure_shade_kernels(int max_dyn_smem) {
     configure_one<NoCount>(max_dyn_smem);
+    configure_one<NoCount3>(max_dyn_smem);
     configure_one<Counts>(max_dyn_smem);
     cudaFuncSetAttribute(k_light_setup<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_light_setup<NoCount3>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
     cudaFuncSetAttribute(k_light_setup<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
     cudaFuncSetAttribute(k_light_compose, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }

@@ -40,12 +40,13 @@ __global__ void __launch_bounds__(128) k_light_surfels(BlobRef blob, SurfelArray
 }
 
 // Loads of data that a kernel itself rewrites between phases (the cluster
-// radiosity vector and the surfels' radiosity in the fused solve) bypass L1
-// (ld.global.cg: L2 is coherent across SMs); the per-bounce kernels, where
-// those arrays are constant for the launch, use the read-only path.
+// radiosity vector and the surfels' radiosity in the fused solve) are plain
+// coherent loads, ordered after the writes by the grid barrier's fences; the
+// per-bounce kernels, where those arrays are constant for the launch, use
+// the read-only path.
 template <bool kFused>
 __device__ __forceinline__ float4 ld_live(const float4* p) {
-    if constexpr (kFused) return __ldcg(p);
+    if constexpr (kFused) return *p;
     else return __ldg(p);
 }
 
@@ -192,6 +193,8 @@ void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_
     const unsigned g = grid_for(n, 128, 16);
     if (counts)
         k_light_surfels<Counts><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, counts, terms);
+    else if (blob.tree3)
+        k_light_surfels<NoCount3><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, nullptr, terms);
     else
         k_light_surfels<NoCount><<<g, 128, blob_smem(blob, 128), st>>>(blob, s, n, evals, status, nullptr, terms);
 }
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(kJacBlock) k_jacobi_sell(float4* direct, float
 }
 
 // solve.rs:47-108 in ONE cooperative launch: every bounce's cluster means
-// (CTA per cluster), a grid barrier, the Jacobi rows (thread per row, the
+// (warp per cluster), a grid barrier, the Jacobi rows (thread per row, the
 // sliced-ELL copy when there is one) with the bounce's residual as an
 // order-free max into its own slot, a second barrier, and the stop test,
 // which every CTA evaluates on the same value. The operations and their
@@ -281,12 +284,33 @@ __global__ void __launch_bounds__(kFusedSolveBlock) k_solve_fused(SurfelArrays s
                                                                    SellMatrix m, float4* cluster_rad,
                                                                    FusedSolve* fs, uint32_t max_bounces,
                                                                    int no_exit, uint32_t* status, uint32_t polls) {
-    __shared__ float4 buf[2][kFusedSolveBlock];
     const int vec = (((uintptr_t)idx | (uintptr_t)w) & 15u) == 0 ? 1 : 0;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     for (uint32_t it = 0; it < max_bounces; ++it) {
-        for (uint32_t c = blockIdx.x; c < nc; c += gridDim.x)
-            cluster_mean<true, kFusedSolveBlock>(s.rad, s.p, cp, crange, members, c, cluster_rad, buf);
+        // Cluster means, a warp per cluster: 32 members' rad * area at a time,
+        // broadcast lane by lane and added in member order.
+        for (uint32_t c = gwarp; c < nc; c += nwarps) {
+            const uint2 r = crange[c];
+            V acc{0.0f, 0.0f, 0.0f};
+            for (uint32_t base = r.x; base < r.y; base += 32u) {
+                const uint32_t k = base + lane;
+                V v{0.0f, 0.0f, 0.0f};
+                if (k < r.y) {
+                    const uint32_t m = __ldg(&members[k]);
+                    const float4 rr = ld_live<true>(&s.rad[m]);
+                    const float a = __ldg(&s.p[m].w);
+                    v = V{rr.x * a, rr.y * a, rr.z * a};
+                }
+                const uint32_t cnt = r.y - base < 32u ? r.y - base : 32u;
+#pragma unroll 4
+                for (uint32_t j = 0; j < cnt; ++j)
+                    acc = acc + V{__shfl_sync(kFull, v.x, j), __shfl_sync(kFull, v.y, j), __shfl_sync(kFull, v.z, j)};
+            }
+            if (lane == 0) cluster_rad[c] = f4(acc / fmaxf(__ldg(&cp[c].w), 1e-12f), 0.0f);
+        }
         if (!grid_barrier(&fs->bar, status, polls)) return;
         float dmax = 0.0f;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -417,6 +441,7 @@ int launch_sell_fill(cudaStream_t st, const uint32_t* starts, const uint32_t* id
 
 void configure_solve_kernels(int max_dyn_smem) {
     cudaFuncSetAttribute(k_light_surfels<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_light_surfels<NoCount3>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
     cudaFuncSetAttribute(k_light_surfels<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }
 

@@ -61,13 +61,16 @@ __global__ void __launch_bounds__(128) k_gen_finalize(BlobRef blob, const float4
 // taken in batches of consecutive indices:
 //   filter   drop seeds that an accepted point of an earlier batch rejects;
 //   append   the rest become this batch's points, in seed order, linked into
-//            their occupancy cells;
+//            the batch's occupancy lists;
 //   resolve  rounds: a point is accepted once every earlier point of the
 //            batch within d_min is rejected, and rejected as soon as one of
 //            them is accepted. Decisions are final and only taken on final
 //            information, so the fixed point is the sequential result and
 //            does not depend on scheduling; each round decides at least the
-//            earliest open point.
+//            earliest open point;
+//   retire   the batch's accepted points join the accepted-point lists that
+//            later filters walk, and the batch lists are emptied, so that no
+//            walk ever passes a rejected point.
 // Lists are walked with a bound (the point capacity); an over-long walk sets
 // kStatusGenWalk.
 __device__ __forceinline__ int gen_cell(const GenGrid& g, float v, int a) {
@@ -79,16 +82,23 @@ __device__ __forceinline__ bool gen_close(float4 a, float4 b, float d2) {
     return dx * dx + dy * dy + dz * dz < d2;
 }
 
-// Visits every point linked into the 27 cells around p: f(index) returns
-// false to stop. Returns false if a walk hit the bound.
+__device__ __forceinline__ size_t gen_cell_index(const GenGrid& g, float4 p) {
+    return (size_t)gen_cell(g, p.x, 0) +
+           (size_t)g.dim[0] * ((size_t)gen_cell(g, p.y, 1) + (size_t)g.dim[1] * gen_cell(g, p.z, 2));
+}
+
+// Visits every point linked into the 27 cells around p in the lists
+// (head, next): f(index) returns false to stop. Returns false if a walk hit
+// the bound.
 template <class F>
-__device__ __forceinline__ bool gen_walk(const GenGrid& g, float4 p, F&& f) {
+__device__ __forceinline__ bool gen_walk(const GenGrid& g, const uint32_t* head, const uint32_t* next, float4 p,
+                                         F&& f) {
     const int cx = gen_cell(g, p.x, 0), cy = gen_cell(g, p.y, 1), cz = gen_cell(g, p.z, 2);
     for (int z = max(cz - 1, 0); z <= min(cz + 1, g.dim[2] - 1); ++z)
         for (int y = max(cy - 1, 0); y <= min(cy + 1, g.dim[1] - 1); ++y)
             for (int x = max(cx - 1, 0); x <= min(cx + 1, g.dim[0] - 1); ++x) {
                 const size_t cell = (size_t)x + (size_t)g.dim[0] * ((size_t)y + (size_t)g.dim[1] * (size_t)z);
-                uint32_t e = g.head[cell];
+                uint32_t e = head[cell];
                 for (uint32_t guard = 0; e != 0; ++guard) {
                     if (guard > g.cap) {
                         atomicOr(g.err, kStatusGenWalk);
@@ -96,19 +106,21 @@ __device__ __forceinline__ bool gen_walk(const GenGrid& g, float4 p, F&& f) {
                     }
                     const uint32_t idx = e - 1;
                     if (!f(idx)) return true;
-                    e = g.next[idx];
+                    e = next[idx];
                 }
             }
     return true;
 }
 
+// A seed survives if no accepted point of an earlier batch lies within d_min
+// (those are exactly the points in the accepted lists).
 __global__ void k_gen_filter(GenGrid g, const float4* cand, uint32_t cnt, uint32_t* keep) {
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
         const float4 q = cand[j];
         bool close = false;
         if (q.w != 0.0f)
-            gen_walk(g, q, [&](uint32_t idx) {
-                if (g.state[idx] == 1u && gen_close(g.pts[idx], q, g.d_min_sq)) close = true;
+            gen_walk(g, g.head_acc, g.next_acc, q, [&](uint32_t idx) {
+                if (gen_close(g.pts[idx], q, g.d_min_sq)) close = true;
                 return !close;
             });
         keep[j] = (q.w != 0.0f && !close) ? 1u : 0u;
@@ -127,9 +139,7 @@ __global__ void k_gen_append(GenGrid g, const float4* cand, const uint32_t* keep
         const float4 q = cand[j];
         g.pts[pid] = q;
         g.state[pid] = 0u;
-        const size_t cell = (size_t)gen_cell(g, q.x, 0) +
-                            (size_t)g.dim[0] * ((size_t)gen_cell(g, q.y, 1) + (size_t)g.dim[1] * gen_cell(g, q.z, 2));
-        g.next[pid] = atomicExch(&g.head[cell], pid + 1u);
+        g.next[pid] = atomicExch(&g.head[gen_cell_index(g, q)], pid + 1u);
     }
 }
 
@@ -141,7 +151,7 @@ __global__ void k_gen_resolve(GenGrid g, uint32_t base, uint32_t count, uint32_t
         if (state[pid] != 0u) continue;
         const float4 p = g.pts[pid];
         bool rej = false, pend = false;
-        const bool ok = gen_walk(g, p, [&](uint32_t idx) {
+        const bool ok = gen_walk(g, g.head, g.next, p, [&](uint32_t idx) {
             if (idx < base || idx >= pid || !gen_close(g.pts[idx], p, g.d_min_sq)) return true;
             const uint32_t s = state[idx];
             if (s == 1u) rej = true;
@@ -166,6 +176,20 @@ __global__ void k_gen_emit(GenGrid g, uint32_t base, uint32_t count, const uint3
                            float4* out) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
         if (g.state[base + k] == 1u && rank[k] < quota) out[rank[k]] = g.pts[base + k];
+}
+
+__global__ void k_gen_retire(GenGrid g, uint32_t base, uint32_t count) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t pid = base + k;
+        const size_t cell = gen_cell_index(g, g.pts[pid]);
+        g.head[cell] = 0u;
+        if (g.state[pid] == 1u) g.next_acc[pid] = atomicExch(&g.head_acc[cell], pid + 1u);
+    }
+}
+
+int launch_gen_retire(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count) {
+    k_gen_retire<<<grid_for(count, 256), 256, 0, st>>>(g, base, count);
+    return 1;
 }
 
 int launch_gen_filter(cudaStream_t st, const GenGrid& g, const float4* cand, uint32_t cnt, uint32_t* keep) {

@@ -162,9 +162,7 @@ __global__ void __launch_bounds__(128) k_closure(BlobRef blob, SceneConsts sc, c
             continue;
         }
         const bool active = item != ~0u;
-        V hp;
-        uint32_t hm;
-        const int st = trace_step_w(sv, ray, active, hp, hm, cnt);
+        const int st = trace_step_dist_w(sv, ray, active, cnt);
         if (active && st != kMarching) {
             clo[item] = (uint16_t)(((st == kMiss) ? 0x100u : 0u) | ray.steps);
             item = ~0u;
@@ -332,6 +330,10 @@ void launch_visibility(cudaStream_t st, BlobRef blob, SceneConsts sc, const floa
     if (counts)
         k_visibility<Counts><<<persistent_grid(k_visibility<Counts>, 128, sm, ncand), 128, sm, st>>>(
             blob, sc, sp, sn, cp, cn, cand_c, cand_row, order, ncand, cand_vis, cand_steps, status, counts, cursor);
+    else if (blob.tree3)
+        k_visibility<NoCount3><<<persistent_grid(k_visibility<NoCount3>, 128, sm, ncand), 128, sm, st>>>(
+            blob, sc, sp, sn, cp, cn, cand_c, cand_row, order, ncand, cand_vis, cand_steps, status, nullptr,
+            cursor);
     else
         k_visibility<NoCount><<<persistent_grid(k_visibility<NoCount>, 128, sm, ncand), 128, sm, st>>>(
             blob, sc, sp, sn, cp, cn, cand_c, cand_row, order, ncand, cand_vis, cand_steps, status, nullptr,
@@ -364,6 +366,9 @@ void launch_closure(cudaStream_t st, BlobRef blob, SceneConsts sc, const float4*
     if (counts)
         k_closure<Counts><<<persistent_grid(k_closure<Counts>, 128, sm, items), 128, sm, st>>>(
             blob, sc, sp, sn, n, order, clo, status, counts, cursor);
+    else if (blob.tree3)
+        k_closure<NoCount3><<<persistent_grid(k_closure<NoCount3>, 128, sm, items), 128, sm, st>>>(
+            blob, sc, sp, sn, n, order, clo, status, nullptr, cursor);
     else
         k_closure<NoCount><<<persistent_grid(k_closure<NoCount>, 128, sm, items), 128, sm, st>>>(
             blob, sc, sp, sn, n, order, clo, status, nullptr, cursor);
@@ -432,8 +437,10 @@ void launch_check_transfer(cudaStream_t st, uint32_t n, uint32_t nc, unsigned lo
 
 void configure_transfer_kernels(int max_dyn_smem) {
     cudaFuncSetAttribute(k_visibility<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_visibility<NoCount3>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
     cudaFuncSetAttribute(k_visibility<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
     cudaFuncSetAttribute(k_closure<NoCount>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
+    cudaFuncSetAttribute(k_closure<NoCount3>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
     cudaFuncSetAttribute(k_closure<Counts>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn_smem);
 }
 

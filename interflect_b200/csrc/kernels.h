@@ -22,6 +22,11 @@ struct BlobRef {
     int staged;
     int stack_depth;  // BVH traversal stack entries per thread (tree depth + 2)
     uint32_t wait_polls;  // poll budget of the staging wait (kDefaultWaitPolls unless the host lowers it)
+    int tree3;            // BVH in use and made of a root and two leaves: the NoCount3 kernels apply
+    // staged == 2: only [0, part_head) (header and objects) and the BVH nodes
+    // [part_nodes_off, + part_nodes) are copied into shared memory.
+    uint32_t part_head, part_nodes_off, part_nodes;
+    LeafGrid lg;          // enabled only for the scenes dist_fast serves (large BVHs)
 };
 
 // Default poll budget of every bounded device-side wait (the scene-staging
@@ -68,8 +73,10 @@ struct GenGrid {
     float inv_cell;
     int dim[3];
     float d_min_sq;
-    uint32_t* head;       // per occupancy cell: 1 + last point inserted, 0 = empty
+    uint32_t* head;       // per occupancy cell: 1 + last point of the current batch inserted, 0 = empty
     uint32_t* next;       // per point: 1 + previous point of its cell, 0 = end
+    uint32_t* head_acc;   // the same lists over the accepted points of all earlier batches
+    uint32_t* next_acc;
     float4* pts;          // points kept after the batch filter, in seed order
     uint32_t* state;      // per point: 0 undecided, 1 accepted, 2 rejected
     uint32_t cap;         // capacity of pts / next / state
@@ -88,6 +95,9 @@ int launch_gen_append(cudaStream_t st, const GenGrid& g, const float4* cand, con
 int launch_gen_resolve(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, uint32_t* undecided);
 int launch_gen_accept_flags(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, uint32_t* flags);
 // out[before + rank] = accepted point, for ranks below quota.
+// After a batch: its accepted points join the accepted lists, and its cells
+// of the batch lists are emptied for the next batch.
+int launch_gen_retire(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count);
 int launch_gen_emit(cudaStream_t st, const GenGrid& g, uint32_t base, uint32_t count, const uint32_t* rank,
                     uint32_t quota, float4* out);
 
@@ -370,6 +380,14 @@ void configure_solve_kernels(int max_dyn_smem);
 void configure_shade_kernels(int max_dyn_smem);
 void configure_diff_kernels(int max_dyn_smem);
 void configure_path_kernels(int max_dyn_smem);
+void configure_leafgrid_kernels(int max_dyn_smem);
+// The leaf grid (k_leafgrid.cu): per-cell bounds U, then the lists (count
+// pass with start == nullptr, fill pass with the scanned starts).
+void launch_lg_bound(cudaStream_t st, const BlobRef& blob, const LeafGrid& g, float cell, float half_diag,
+                     uint32_t ncells, float* U, uint32_t* status);
+void launch_lg_lists(cudaStream_t st, const uint8_t* blob, const LeafGrid& g, double cell, double pad, uint32_t ncells,
+                     const float* U, const uint32_t* leaves, uint32_t nleaf, uint32_t* count, const uint32_t* start,
+                     uint32_t* out, float* key);
 // The path-traced reference mode (k_path.cu): p.film / p.out8 receive the
 // frame; sincos holds (sinf, cosf) of the 2^24 sampler angles.
 int launch_path(cudaStream_t st, const ShadeParams& p, uint32_t spp, const float2* sincos,
@@ -381,6 +399,7 @@ inline void configure_kernels(int max_dyn_smem) {
     configure_shade_kernels(max_dyn_smem);
     configure_diff_kernels(max_dyn_smem);
     configure_path_kernels(max_dyn_smem);
+    configure_leafgrid_kernels(max_dyn_smem);
 }
 
 }  // namespace ifx

@@ -90,6 +90,22 @@ struct alignas(16) BlobHeader {
     uint32_t off_sphere_lights, off_materials, off_linear, total_bytes;
 };
 
+// Candidate leaves per cell of a uniform grid over the scene, used by the
+// distance-only queries of cone-shadow marches in large BVHs (device.cuh,
+// dist_fast). A cell lists every BVH leaf whose box comes within
+// U(cell) + 2 tol of the cell, U(cell) being the reference's distance at the
+// cell centre plus the cell's half-diagonal (an upper bound of the nearest
+// distance anywhere in the cell); leaves appear nearest-first.
+struct LeafGrid {
+    const uint32_t* start;  // per cell: first entry of its list; start[ncells] = total
+    const uint32_t* leaf;   // BVH node index of each listed leaf
+    float lo[3];
+    float inv_cell;
+    int dim[3];
+    float tol;              // pruning margin, far above any f32 rounding of the distances
+    int enabled;
+};
+
 // Per-scene scalars passed to kernels by value.
 struct SceneConsts {
     float lo[3], hi[3];
