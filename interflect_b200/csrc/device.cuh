@@ -331,10 +331,21 @@ __device__ __forceinline__ float prim_dist(const DPrim& pr, V p, C& cnt) {
     return kMaxF;
 }
 
-// sdf.rs:166-172 with the smooth-subtraction extension.
+// sdf.rs:166-172 with the smooth-subtraction extension. `best` is the
+// caller's best distance so far, against which the result is only compared
+// with a strict `<`. A subtraction never lowers the base primitive's
+// distance: max(d, -s) >= d exactly, and the smooth form is above max(d, -s)
+// but for rounding (a few ulps of its operands, far below the margin here).
+// So in the uncounted kernels, a base at or beyond `best` (plus that margin
+// for the smooth form) cannot win the comparison, and its subtractions are
+// not evaluated; the returned value is then the base's, itself >= best. The
+// counting kernels evaluate everything, as the reference does.
 template <class C>
-__device__ __forceinline__ float obj_dist(const SceneView& sv, const DObject& o, V p, C& cnt) {
+__device__ __forceinline__ float obj_dist(const SceneView& sv, const DObject& o, V p, C& cnt, float best = kMaxF) {
     float d = prim_dist(sv.prim(o.prim), p, cnt);
+    if constexpr (sizeof(C) == 1) {
+        if (o.nsub > 0 && d >= best + (o.smooth > 0.0f ? 1e-5f * (1.0f + fabsf(best) + o.smooth) : 0.0f)) return d;
+    }
     for (int s = 1; s <= o.nsub; ++s) {
         float sd = prim_dist(sv.prim(o.prim + s), p, cnt);
         cnt.add(o.smooth > 0.0f ? CN_SMOOTH : CN_HARD);
@@ -371,7 +382,7 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
     DistHit best{kMaxF, 0u};
     for (int i = 0; i < sv.n_planes; ++i) {
         const DObject o = sv.obj(i);
-        float d = obj_dist(sv, o, p, cnt);
+        float d = obj_dist(sv, o, p, cnt, best.d);
         if (d < best.d) best = DistHit{d, o.mat};
     }
     if constexpr (C::kTree3) {
@@ -388,7 +399,7 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
             const DNode& nd = sv.node(left ? 1 : r);
             for (int k = nd.link; k < nd.link + nd.count; ++k) {
                 const DObject o = sv.obj(k);
-                const float d = obj_dist(sv, o, p, cnt);
+                const float d = obj_dist(sv, o, p, cnt, best.d);
                 if (d < best.d) {
                     best.d = d;
                     best.mat = o.mat;
@@ -422,7 +433,7 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
             if (nd.count > 0) {
                 for (int k = nd.link; k < nd.link + nd.count; ++k) {
                     const DObject o = sv.obj(k);
-                    float d = obj_dist(sv, o, p, cnt);
+                    float d = obj_dist(sv, o, p, cnt, best.d);
                     if (d < best.d) {
                         best.d = d;
                         best.mat = o.mat;
@@ -454,7 +465,7 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
     } else {
         for (int k = 0; k < sv.n_objects; ++k) {
             const DObject o = sv.obj(sv.lin(k));
-            float d = obj_dist(sv, o, p, cnt);
+            float d = obj_dist(sv, o, p, cnt, best.d);
             if (d < best.d) {
                 best.d = d;
                 best.mat = o.mat;
@@ -475,7 +486,7 @@ __device__ __forceinline__ void leaf_eval(const SceneView& sv, int leaf, V p, Di
     const DNode nd = sv.node(leaf);
     for (int k = nd.link; k < nd.link + nd.count; ++k) {
         const DObject o = sv.obj(k);
-        const float d = obj_dist(sv, o, p, cnt);
+        const float d = obj_dist(sv, o, p, cnt, best.d);
         if (d < best.d) {
             best.d = d;
             best.mat = o.mat;
@@ -543,7 +554,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         cnt.add(CN_SDF);
         for (int i = 0; i < sv.n_planes; ++i) {
             const DObject o = sv.obj(i);
-            float d = obj_dist(sv, o, p, cnt);
+            float d = obj_dist(sv, o, p, cnt, best.d);
             if (d < best.d) best = DistHit{d, o.mat};
         }
     }
@@ -552,7 +563,7 @@ __device__ __forceinline__ DistHit dist_mat_warp(const SceneView& sv, V p, bool 
         if (active) {
             for (int k = 0; k < sv.n_objects; ++k) {
                 const DObject o = sv.obj(sv.lin(k));
-                float d = obj_dist(sv, o, p, cnt);
+                float d = obj_dist(sv, o, p, cnt, best.d);
                 if (d < best.d) {
                     best.d = d;
                     best.mat = o.mat;
