@@ -802,6 +802,9 @@ __device__ __forceinline__ int trace_step(const SceneView& sv, TraceRay& r, V& p
 //    unless it prunes L1 or an ancestor, which needs a best <= box(L1) first;
 //    so G is its answer when G is a plane's, when box(L1) <= G, or when no
 //    other leaf or plane reaches box(L1) (then nothing can have pruned L1).
+// At or inside a surface (G <= 0) the value may differ from the reference's
+// but both are below every stopping threshold of the marches that use it
+// (shadow 1e-4, trace 1e-4 * max(t, 1)), so the march ends at the same step.
 // Otherwise (and outside the grid) ok is false and the caller asks the
 // reference query.
 __device__ __forceinline__ float dist_fast(const SceneView& sv, V p, bool& ok) {
@@ -840,9 +843,13 @@ __device__ __forceinline__ float dist_fast(const SceneView& sv, V p, bool& ok) {
         }
         if (m < best) best = m;
     }
-    if (P <= m1) {
+    const float G = P <= m1 ? P : m1;
+    // At or inside a surface: the reference's value is <= 0 too, or within
+    // rounding of it (a leaf can only be pruned against a best <= its box
+    // distance, which is ~0 here), so both stop the march at this step.
+    if (G <= 0.0f || P <= m1) {
         ok = true;
-        return P;
+        return G;
     }
     const float v1 = sqrtf(d2_1);
     ok = v1 <= m1 || (m2 > v1 && P > v1);

@@ -54,7 +54,9 @@ __global__ void k_lg_lists(const uint8_t* blob, LeafGrid g, double cell, double 
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
         uint32_t x, y, z;
         lg_cell(g, c, x, y, z);
-        const double lim = (double)U[c] + 2.0 * (double)g.tol;
+        // Inside an object U can be negative while the box holding the point
+        // is at distance 0: the bound is taken against 0 at least.
+        const double lim = fmax((double)U[c], 0.0) + 2.0 * (double)g.tol;
         uint32_t n = 0;
         const uint32_t o = start ? start[c] : 0u;
         for (uint32_t i = 0; i < nleaf; ++i) {
