@@ -169,11 +169,10 @@ int ifx_timer_stop(ifx_ctx* ctx, float* ms);
  * Default 24 KiB, at most 128 KiB. No counterpart in the reference. */
 int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes);
 /* Failure detection: the poll budget of this context's bounded device-side
- * waits (the scene-staging wait of every ray-marching kernel and the grid
- * barrier of the one-launch solve). A wait that runs out of polls sets a
- * status bit, leaves its kernel without tracing (after its own copy in
- * flight has landed), and the call returns IFX_ERR_TIMEOUT; the context
- * stays usable. 0 polls makes every such wait give up at once; the default
+ * waits (the scene-staging wait of every ray-marching kernel). A wait that
+ * runs out of polls sets a status bit, leaves its kernel without tracing
+ * (after its own copy in flight has landed), and the call returns
+ * IFX_ERR_TIMEOUT; the context stays usable. 0 polls makes every such wait give up at once; the default
  * is IFX_WAIT_LIMIT_DEFAULT. Lowering it is for tests of that error path.
  * No counterpart in the reference, whose stages cannot fail (it only
  * validates input, src/scene.rs:106-148). */
@@ -418,6 +417,15 @@ int ifx_multiscene_add(ifx_multiscene* ms, ifx_ctx* ctx, const ifx_camera* cam, 
  * choice never changes a bit) and captures the CUDA graph. grid and block
  * (nullable) receive the chosen shape. */
 int ifx_multiscene_build(ifx_multiscene* ms, int autotune, int* grid, int* block);
+/* Failure detection: the poll budget of each grid barrier of the packed
+ * launch (default IFX_MULTISCENE_WAIT_DEFAULT), taking effect at the next
+ * ifx_multiscene_build. A barrier that runs out makes ifx_multiscene_run
+ * return IFX_ERR_TIMEOUT and leaves the packed frame usable; 0 makes every
+ * barrier give up at once, for tests of that path. No counterpart in the
+ * reference. */
+#define IFX_MULTISCENE_WAIT_DEFAULT (1u << 24)
+int ifx_multiscene_set_wait_limit(ifx_multiscene* ms, uint32_t polls);
+
 /* One graph launch: every scene's frame. ms_out (nullable): CUDA-event time. */
 int ifx_multiscene_run(ifx_multiscene* ms, float* ms_out);
 /* Scene `index` of the last run: linear film (w*h*3 f32), encoded frame

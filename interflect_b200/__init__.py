@@ -37,12 +37,13 @@ COMPARE_PATH = os.path.join(_HERE, "bin", "compare")
 
 IFX_OK, IFX_ERR_INVALID, IFX_ERR_PARSE, IFX_ERR_CUDA, IFX_ERR_NOMEM, IFX_ERR_LIMIT, IFX_ERR_TIMEOUT = range(7)
 WAIT_LIMIT_DEFAULT = 1 << 22  # IFX_WAIT_LIMIT_DEFAULT
+MULTISCENE_WAIT_DEFAULT = 1 << 24  # IFX_MULTISCENE_WAIT_DEFAULT
 MODES = {"beauty": 0, "direct": 1, "indirect": 2, "normals": 3, "depth": 4, "steps": 5}
 
 # Every symbol include/interflect.h declares.
 EXPORTS = (
     "ifx_scene_parse", "ifx_scene_free", "ifx_scene_get_info", "ifx_scene_set_cfg", "ifx_scene_set_use_bvh",
-    "ifx_scene_get_bvh", "ifx_set_wait_limit", "ifx_set_leaf_grid",
+    "ifx_scene_get_bvh", "ifx_set_wait_limit", "ifx_set_leaf_grid", "ifx_multiscene_set_wait_limit",
     "ifx_ctx_create", "ifx_ctx_destroy", "ifx_last_error", "ifx_get_stats", "ifx_scene_upload",
     "ifx_surfels_generate", "ifx_surfels_upload", "ifx_surfels_count", "ifx_surfels_download",
     "ifx_transfer_build", "ifx_transfer_download", "ifx_clusters_download", "ifx_transfer_row_diag",
@@ -185,6 +186,7 @@ def lib() -> C.CDLL:
         "ifx_set_stage_limit": (I, [P, U32]),
         "ifx_set_wait_limit": (I, [P, U32]),
         "ifx_set_leaf_grid": (I, [P, I]),
+        "ifx_multiscene_set_wait_limit": (I, [P, U32]),
         "ifx_clusters_build": (I, [P, I, C.POINTER(U64)]),
         "ifx_render_reference": (I, [P, C.POINTER(_Camera), U32, U32, U32, F, P, P]),
         "ifx_frame": (I, [P, I, U32, C.POINTER(_Camera), I, U32, U32, F, P, P, C.POINTER(_FrameInfo)]),
@@ -684,6 +686,8 @@ class MultiScene:
             msg = lib().ifx_multiscene_last_error(self._h).decode(errors="replace")
             if r == IFX_ERR_LIMIT:
                 raise LimitError(f"{what}: {msg}")
+            if r == IFX_ERR_TIMEOUT:
+                raise WaitTimeout(f"{what} failed ({r}): {msg}")
             raise DeviceError(f"{what} failed ({r}): {msg}")
 
     def add(self, ctx: Context, width: int, height: int, max_bounces: int, cam=None) -> int:
@@ -692,6 +696,12 @@ class MultiScene:
                                              height, max_bounces, C.byref(i)), "multiscene add")
         self._members.append((ctx, width, height))
         return i.value
+
+    def set_wait_limit(self, polls: int | None) -> None:
+        """Poll budget of the packed launch's grid barriers from the next
+        build (None: the default); 0 makes each barrier give up at once."""
+        self._check(lib().ifx_multiscene_set_wait_limit(self._h, MULTISCENE_WAIT_DEFAULT if polls is None else polls),
+                    "set_wait_limit")
 
     def build(self, autotune: bool = True) -> tuple[int, int]:
         g, b = C.c_int(), C.c_int()

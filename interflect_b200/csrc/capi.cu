@@ -2,6 +2,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -83,7 +84,11 @@ struct ifx_ctx {
 
     // solve
     DBuf cluster_rad, ctl;
-    DBuf fsolve;  // FusedSolve block of the one-launch solve
+    // the solve's launch sequence as a graph, and the buffers and sizes it was captured for
+    cudaGraph_t solve_graph = nullptr;
+    cudaGraphExec_t solve_exec = nullptr;
+    std::array<uintptr_t, 24> solve_graph_key{};
+    uint64_t solve_graph_launches = 0;
     // poll budget of the bounded device-side waits (staging, grid barrier)
     uint32_t wait_polls = kDefaultWaitPolls;
     // the transfer in sliced-ELL form for the solve (built with the transfer)
@@ -417,6 +422,7 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
 }
 
 static void multiscene_forget(ifx_multiscene* ms, ifx_ctx* ctx);
+static void solve_graph_drop(ifx_ctx* ctx);
 
 extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     if (!ctx) return;
@@ -425,6 +431,7 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     if (ctx->st2) cudaStreamSynchronize(ctx->st2);
     if (ctx->st3) cudaStreamSynchronize(ctx->st3);
+    solve_graph_drop(ctx);
     DBuf* bufs[] = {&ctx->blob, &ctx->status, &ctx->srgb_t, &ctx->sp, &ctx->sn, &ctx->salb, &ctx->sdir, &ctx->sirr,
                     &ctx->srad, &ctx->keys, &ctx->keys_alt, &ctx->heads, &ctx->head_scan, &ctx->seg_start,
                     &ctx->members, &ctx->cp_tmp, &ctx->cn_tmp, &ctx->valid, &ctx->valid_scan, &ctx->cp, &ctx->cn,
@@ -445,7 +452,7 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->sell_rows, &ctx->sell_sizes, &ctx->sell_off, &ctx->sell_idx, &ctx->sell_w,
                     &ctx->path_sincos, &ctx->shsc, &ctx->lff, &ctx->lvis, &ctx->lq, &ctx->lsc,
                     &ctx->vkey, &ctx->vkey_alt, &ctx->vval, &ctx->vval_alt, &ctx->ckey, &ctx->ckey_alt,
-                    &ctx->cval, &ctx->cval_alt, &ctx->fsolve, &ctx->msum, &ctx->gen_head_acc, &ctx->gen_next_acc, &ctx->lg_U, &ctx->lg_count,
+                    &ctx->cval, &ctx->cval_alt, &ctx->msum, &ctx->gen_head_acc, &ctx->gen_next_acc, &ctx->lg_U, &ctx->lg_count,
                     &ctx->lg_start, &ctx->lg_leaves, &ctx->lg_leaf, &ctx->lg_key};
     for (DBuf* b : bufs) free_buf(*b);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -1372,6 +1379,42 @@ extern "C" int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals) {
     return IFX_OK;
 }
 
+// The solve's launch sequence depends only on these buffers and sizes; while
+// they stay the same the sequence is replayed from a captured CUDA graph.
+static std::array<uintptr_t, 24> solve_key(ifx_ctx* ctx, uint32_t max_bounces) {
+    const SurfelArrays s = ctx->sarr();
+    const SellMatrix& m = ctx->sellm;
+    const bool sell = ctx->sell_ready;
+    return {(uintptr_t)s.p, (uintptr_t)s.albedo, (uintptr_t)s.direct, (uintptr_t)s.irr, (uintptr_t)s.rad,
+            (uintptr_t)ctx->cp.p, (uintptr_t)ctx->crange.p, (uintptr_t)ctx->members.p, (uintptr_t)ctx->starts.p,
+            (uintptr_t)ctx->idx.p, (uintptr_t)ctx->w.p, (uintptr_t)ctx->cluster_rad.p, (uintptr_t)ctx->ctl.p,
+            sell ? (uintptr_t)m.perm : 0, sell ? (uintptr_t)m.len : 0, sell ? (uintptr_t)m.slice_off : 0,
+            sell ? (uintptr_t)m.idx : 0, sell ? (uintptr_t)m.w : 0, (uintptr_t)ctx->n, (uintptr_t)ctx->nc,
+            (uintptr_t)max_bounces, 1u, 0u, 0u};
+}
+
+static void solve_graph_drop(ifx_ctx* ctx) {
+    if (ctx->solve_exec) cudaGraphExecDestroy(ctx->solve_exec);
+    if (ctx->solve_graph) cudaGraphDestroy(ctx->solve_graph);
+    ctx->solve_exec = nullptr;
+    ctx->solve_graph = nullptr;
+}
+
+// Enqueues the control-block reset and max_bounces bounces (three launches
+// each) on ctx->st; bounces after convergence return at once on the
+// device-side flag.
+static void solve_enqueue(ifx_ctx* ctx, uint32_t first, uint32_t end) {
+    SolveCtl* ctl = (SolveCtl*)ctx->ctl.p;
+    for (uint32_t it = first; it < end; ++it) {
+        int l = 0;
+        launch_solve_bounce(ctx->st, ctx->sarr(), ctx->n, (const float4*)ctx->cp.p, (const uint2*)ctx->crange.p,
+                            (const uint32_t*)ctx->members.p, ctx->nc, (const uint32_t*)ctx->starts.p,
+                            (const uint32_t*)ctx->idx.p, (const float*)ctx->w.p, (float4*)ctx->cluster_rad.p, ctl, it,
+                            &l, 0, ctx->sell_ready ? &ctx->sellm : nullptr);
+        ctx->launches += (uint64_t)l;
+    }
+}
+
 extern "C" int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* out) {
     if (!ctx || !ctx->has_transfer) return fail(ctx, IFX_ERR_INVALID, "no transfer");
     CK(cudaSetDevice(ctx->device));
@@ -1380,40 +1423,47 @@ extern "C" int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* ou
         return IFX_OK;
     }
     ENSURE(ctx->cluster_rad, (size_t)ctx->nc * 16);
+    SolveCtl* ctl = (SolveCtl*)ctx->ctl.p;
     SolveCtl h{};
-    const SellMatrix* sell = ctx->sell_ready ? &ctx->sellm : nullptr;
-    // Up to kFusedSolveMaxRows rows the solve is latency-bound (a few
-    // microseconds of work per bounce): all bounces run in one cooperative
-    // launch. Larger systems are bandwidth-bound and take one launch per
-    // phase, where launch overhead is negligible.
-    const int fgrid = ctx->n <= kFusedSolveMaxRows && max_bounces <= kFusedSolveMaxBounces
-                          ? fused_solve_grid(ctx->n, ctx->nc, sell != nullptr)
-                          : 0;
-    if (fgrid > 0) {
-        ENSURE(ctx->fsolve, sizeof(FusedSolve));
-        FusedSolve* fs = (FusedSolve*)ctx->fsolve.p;
-        CK(cudaMemsetAsync(fs, 0, sizeof(FusedSolve), ctx->st));
-        CK(cudaEventRecord(ctx->ev0, ctx->st));
-        if (max_bounces > 0) {
-            if (launch_solve_fused(ctx->st, fgrid, ctx->sarr(), ctx->n, (const float4*)ctx->cp.p,
-                                   (const uint2*)ctx->crange.p, (const uint32_t*)ctx->members.p, ctx->nc,
-                                   (const uint32_t*)ctx->starts.p, (const uint32_t*)ctx->idx.p,
-                                   (const float*)ctx->w.p, sell, (float4*)ctx->cluster_rad.p, fs, max_bounces, 0,
-                                   (uint32_t*)ctx->status.p, ctx->wait_polls) < 0) {
-                cudaGetLastError();
-                return fail(ctx, IFX_ERR_CUDA, "cooperative launch of the solve was refused");
+    // Up to kSolveGraphBounces the whole sequence (the bounces after
+    // convergence are no-ops) is one graph launch: the host neither issues
+    // three launches per bounce nor looks at the flag in between.
+    const uint32_t kSolveGraphBounces = 64;
+    bool graphed = false;
+    if (max_bounces > 0 && max_bounces <= kSolveGraphBounces) {
+        const auto key = solve_key(ctx, max_bounces);
+        if (!ctx->solve_exec || key != ctx->solve_graph_key) {
+            solve_graph_drop(ctx);
+            const uint64_t l0 = ctx->launches;
+            if (cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                cudaMemsetAsync(ctl, 0, sizeof(SolveCtl), ctx->st);
+                solve_enqueue(ctx, 0, max_bounces);
+                cudaGraph_t g = nullptr;
+                cudaError_t ce = cudaStreamEndCapture(ctx->st, &g);
+                cudaGraphExec_t x = nullptr;
+                if (ce == cudaSuccess && g && cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+                    ctx->solve_graph = g;
+                    ctx->solve_exec = x;
+                    ctx->solve_graph_key = key;
+                    ctx->solve_graph_launches = ctx->launches - l0;
+                } else if (g) {
+                    cudaGraphDestroy(g);
+                }
             }
-            ctx->launches++;
+            ctx->launches = l0;
+            cudaGetLastError();
         }
-        CK(cudaEventRecord(ctx->ev1, ctx->st));
-        uint32_t hv[4];
-        CK(cudaMemcpyAsync(hv, &fs->iterations, 16, cudaMemcpyDeviceToHost, ctx->st));
-        int r = check_status(ctx);
-        if (r) return r;
-        h.iterations = hv[0];
-        h.last_residual = hv[1];
-    } else {
-        SolveCtl* ctl = (SolveCtl*)ctx->ctl.p;
+        if (ctx->solve_exec) {
+            CK(cudaEventRecord(ctx->ev0, ctx->st));
+            CK(cudaGraphLaunch(ctx->solve_exec, ctx->st));
+            CK(cudaEventRecord(ctx->ev1, ctx->st));
+            CK(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            ctx->launches += ctx->solve_graph_launches;
+            graphed = true;
+        }
+    }
+    if (!graphed) {
         CK(cudaMemsetAsync(ctl, 0, sizeof(SolveCtl), ctx->st));
         CK(cudaEventRecord(ctx->ev0, ctx->st));
         // Bounces are enqueued in batches; the host looks at the device-side
@@ -1421,14 +1471,8 @@ extern "C" int ifx_solve(ifx_ctx* ctx, uint32_t max_bounces, ifx_solve_stats* ou
         const uint32_t kBatch = 16;
         for (uint32_t it = 0; it < max_bounces;) {
             uint32_t end = it + kBatch < max_bounces ? it + kBatch : max_bounces;
-            for (; it < end; ++it) {
-                int l = 0;
-                launch_solve_bounce(ctx->st, ctx->sarr(), ctx->n, (const float4*)ctx->cp.p,
-                                    (const uint2*)ctx->crange.p, (const uint32_t*)ctx->members.p, ctx->nc,
-                                    (const uint32_t*)ctx->starts.p, (const uint32_t*)ctx->idx.p,
-                                    (const float*)ctx->w.p, (float4*)ctx->cluster_rad.p, ctl, it, &l, 0, sell);
-                ctx->launches += (uint64_t)l;
-            }
+            solve_enqueue(ctx, it, end);
+            it = end;
             CKL();
             CK(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, ctx->st));
             CK(cudaStreamSynchronize(ctx->st));
@@ -2184,6 +2228,7 @@ struct ifx_multiscene {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int grid = 0, block = 0;
+    uint32_t wait_polls = IFX_MULTISCENE_WAIT_DEFAULT;  // grid-barrier budget, fixed at build
 };
 
 static void multiscene_forget(ifx_multiscene* ms, ifx_ctx* ctx) {
@@ -2369,6 +2414,12 @@ static int ms_check(ifx_multiscene* ms) {
     return IFX_OK;
 }
 
+extern "C" int ifx_multiscene_set_wait_limit(ifx_multiscene* ms, uint32_t polls) {
+    if (!ms) return IFX_ERR_INVALID;
+    ms->wait_polls = polls;
+    return IFX_OK;
+}
+
 static int ms_launch(ifx_multiscene* ms, cudaGraphExec_t x, float* ms_out) {
     MSCK(cudaEventRecord(ms->e0, ms->st));
     MSCK(cudaGraphLaunch(x, ms->st));
@@ -2439,6 +2490,7 @@ extern "C" int ifx_multiscene_build(ifx_multiscene* ms, int autotune, int* grid_
     p.bar = (MsBarrier*)ms->bar.p;
     p.status = (uint32_t*)ms->status.p;
     p.srgb_t = (const float*)ms->srgb_t.p;
+    p.polls = ms->wait_polls;
     // Launch shapes: block size x CTAs per SM, never above what is resident.
     struct Shape {
         int grid, block;

@@ -25,23 +25,7 @@ __global__ void __launch_bounds__(256) k_agg_batched(const float4* rad, const fl
         if (r >= R || done[r]) continue;
         const uint2 rg = crange[c];
         V acc{0.0f, 0.0f, 0.0f};
-        uint32_t k = rg.x;
-        // Eight members' loads in flight before their ordered adds.
-        for (; k + 8 <= rg.y; k += 8) {
-            uint32_t m[8];
-            float a[8];
-            float4 v[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) m[j] = __ldg(&members[k + j]);
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                a[j] = __ldg(&sp[m[j]].w);
-                v[j] = rad[(size_t)m[j] * R + r];
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc = acc + mk4(v[j]) * a[j];
-        }
-        for (; k < rg.y; ++k) {
+        for (uint32_t k = rg.x; k < rg.y; ++k) {
             const uint32_t m = __ldg(&members[k]);
             const float a = __ldg(&sp[m].w);
             acc = acc + mk4(rad[(size_t)m * R + r]) * a;
@@ -66,24 +50,8 @@ __global__ void __launch_bounds__(512) k_spmm(const float4* direct, const float4
         for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
             V acc{0.0f, 0.0f, 0.0f};
             const uint32_t e = starts[i + 1];
-            uint32_t k = starts[i];
-            // Eight links' index, weight and cluster-value loads in flight
-            // before their adds, which stay in CSR order.
-            for (; k + 8 <= e; k += 8) {
-                uint32_t ci[8];
-                float wv[8];
-                float4 cv[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    ci[j] = __ldg(&idx[k + j]);
-                    wv[j] = __ldg(&w[k + j]);
-                }
-#pragma unroll
-                for (int j = 0; j < 8; ++j) cv[j] = crad[(size_t)ci[j] * R + r];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc = acc + mk4(cv[j]) * wv[j];
-            }
-            for (; k < e; ++k) acc = acc + mk4(crad[(size_t)__ldg(&idx[k]) * R + r]) * __ldg(&w[k]);
+            for (uint32_t k = starts[i]; k < e; ++k)
+                acc = acc + mk4(crad[(size_t)__ldg(&idx[k]) * R + r]) * __ldg(&w[k]);
             const size_t o = (size_t)i * R + r;
             const V nr = mk4(direct[o]) + mk4(__ldg(&albedo[i])) * acc;
             const V diff = vabs(nr - mk4(rad[o]));

@@ -23,8 +23,6 @@
 
 namespace ifx {
 
-static constexpr uint32_t kBarrierPolls = 1u << 24;
-
 // Scene owning packed item `item`: the last scene whose base is <= item.
 __device__ __forceinline__ int scene_of(const uint32_t* base, int S, uint32_t item) {
     int lo = 0, hi = S - 1;
@@ -60,7 +58,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
         S.rad[i] = f4(out, 0.0f);
         S.irr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
-    if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
+    if (!grid_barrier(M.bar, M.status, M.polls)) return;
 
     for (uint32_t it = 0; it < M.max_bounces; ++it) {
         // solve.rs:61-73: cluster means, members summed in member order.
@@ -79,7 +77,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
             }
             S.crad[c] = f4(acc / fmaxf(S.cp[c].w, 1e-12f), 0.0f);
         }
-        if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
+        if (!grid_barrier(M.bar, M.status, M.polls)) return;
         // solve.rs:76-102: Jacobi rows; the residual is the per-scene max.
         for (uint32_t item = tid; item < M.total_surf; item += stride) {
             const int s = scene_of(M.surf_base, M.S, item);
@@ -102,7 +100,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
             bits = __reduce_max_sync(grp, bits);
             if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && bits) atomicMax(&M.ctl[s].residual_bits, bits);
         }
-        if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
+        if (!grid_barrier(M.bar, M.status, M.polls)) return;
         // solve.rs:454-462 per scene, with each scene's own bounce cap.
         if (blockIdx.x == 0) {
             __shared__ uint32_t live;
@@ -121,7 +119,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
             __syncthreads();
             if (threadIdx.x == 0) M.live[0] = live;
         }
-        if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
+        if (!grid_barrier(M.bar, M.status, M.polls)) return;
         if (*(volatile uint32_t*)&M.live[0] == 0) break;
     }
 
@@ -131,7 +129,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
         const uint32_t k = item - S.surf_base;
         S.girr[k] = S.irr[S.gitems[k]];
     }
-    if (!grid_barrier(M.bar, M.status, kBarrierPolls)) return;
+    if (!grid_barrier(M.bar, M.status, M.polls)) return;
 
     // main.rs:289-358 for every pixel of every scene.
     NoCount cnt;

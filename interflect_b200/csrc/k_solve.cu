@@ -39,23 +39,12 @@ __global__ void __launch_bounds__(128) k_light_surfels(BlobRef blob, SurfelArray
     if constexpr (sizeof(C) > 1) cnt.flush(counts);
 }
 
-// Loads of data that a kernel itself rewrites between phases (the cluster
-// radiosity vector and the surfels' radiosity in the fused solve) are plain
-// coherent loads, ordered after the writes by the grid barrier's fences; the
-// per-bounce kernels, where those arrays are constant for the launch, use
-// the read-only path.
-template <bool kFused>
-__device__ __forceinline__ float4 ld_live(const float4* p) {
-    if constexpr (kFused) return *p;
-    else return __ldg(p);
-}
-
 // solve.rs:61-73: cluster radiosity as the area-weighted mean of its
 // members' radiosity, summed sequentially in member order, by one CTA: the
 // threads gather members' rad * area (each product exact per element) into
 // shared memory chunk by chunk, double-buffered, and thread 0 adds them in
 // member order.
-template <bool kFused, int kBlock>
+template <int kBlock>
 __device__ __forceinline__ void cluster_mean(const float4* rad, const float4* sp, const float4* cp,
                                              const uint2* crange, const uint32_t* members, uint32_t c,
                                              float4* cluster_rad, float4 (*buf)[kBlock]) {
@@ -66,7 +55,7 @@ __device__ __forceinline__ void cluster_mean(const float4* rad, const float4* sp
         uint32_t k = r.x + ch * kBlock + threadIdx.x;
         if (k < r.y) {
             uint32_t m = __ldg(&members[k]);
-            float4 v = ld_live<kFused>(&rad[m]);
+            float4 v = __ldg(&rad[m]);
             float a = __ldg(&sp[m].w);
             buf[b][threadIdx.x] = make_float4(v.x * a, v.y * a, v.z * a, 0.0f);
         }
@@ -109,7 +98,7 @@ __global__ void __launch_bounds__(kAggBlock) k_cluster_agg(const float4* rad, co
     if (ctl->done) return;
     __shared__ float4 buf[2][kAggBlock];
     for (uint32_t c = blockIdx.x; c < nc; c += gridDim.x)
-        cluster_mean<false, kAggBlock>(rad, sp, cp, crange, members, c, cluster_rad, buf);
+        cluster_mean<kAggBlock>(rad, sp, cp, crange, members, c, cluster_rad, buf);
 }
 
 // solve.rs:76-102: one Jacobi row per thread, its links added in CSR order
@@ -122,21 +111,20 @@ __global__ void __launch_bounds__(kAggBlock) k_cluster_agg(const float4* rad, co
 // maximum change over rows, an order-free reduction kept as the bits of a
 // non-negative f32 (NaN ignored, as the reference's f32::max fold does).
 static constexpr int kJacBlock = 256;
-template <bool kFused>
 __device__ __forceinline__ V jacobi_row(const float4* crad, const uint32_t* __restrict__ idx,
                                         const float* __restrict__ w, uint32_t k, uint32_t e, int vec) {
     V irr{0.0f, 0.0f, 0.0f};
     if (vec) {
-        for (; k < e && (k & 3u); ++k) irr = irr + mk4(ld_live<kFused>(&crad[__ldg(&idx[k])])) * __ldg(&w[k]);
+        for (; k < e && (k & 3u); ++k) irr = irr + mk4(__ldg(&crad[__ldg(&idx[k])])) * __ldg(&w[k]);
         for (; k + 8 <= e; k += 8) {
             const uint4 i0 = __ldg(reinterpret_cast<const uint4*>(idx + k));
             const uint4 i1 = __ldg(reinterpret_cast<const uint4*>(idx + k + 4));
             const float4 w0 = __ldg(reinterpret_cast<const float4*>(w + k));
             const float4 w1 = __ldg(reinterpret_cast<const float4*>(w + k + 4));
-            const float4 c0 = ld_live<kFused>(&crad[i0.x]), c1 = ld_live<kFused>(&crad[i0.y]),
-                         c2 = ld_live<kFused>(&crad[i0.z]), c3 = ld_live<kFused>(&crad[i0.w]),
-                         c4 = ld_live<kFused>(&crad[i1.x]), c5 = ld_live<kFused>(&crad[i1.y]),
-                         c6 = ld_live<kFused>(&crad[i1.z]), c7 = ld_live<kFused>(&crad[i1.w]);
+            const float4 c0 = __ldg(&crad[i0.x]), c1 = __ldg(&crad[i0.y]),
+                         c2 = __ldg(&crad[i0.z]), c3 = __ldg(&crad[i0.w]),
+                         c4 = __ldg(&crad[i1.x]), c5 = __ldg(&crad[i1.y]),
+                         c6 = __ldg(&crad[i1.z]), c7 = __ldg(&crad[i1.w]);
             irr = irr + mk4(c0) * w0.x;
             irr = irr + mk4(c1) * w0.y;
             irr = irr + mk4(c2) * w0.z;
@@ -147,16 +135,15 @@ __device__ __forceinline__ V jacobi_row(const float4* crad, const uint32_t* __re
             irr = irr + mk4(c7) * w1.w;
         }
     }
-    for (; k < e; ++k) irr = irr + mk4(ld_live<kFused>(&crad[__ldg(&idx[k])])) * __ldg(&w[k]);
+    for (; k < e; ++k) irr = irr + mk4(__ldg(&crad[__ldg(&idx[k])])) * __ldg(&w[k]);
     return irr;
 }
 
 // The CSR row i of one bounce: irradiance, new radiosity, |change|.
-template <bool kFused>
 __device__ __forceinline__ float csr_row_update(float4* direct, float4* albedo, float4* irr_out, float4* rad,
                                                 const uint32_t* starts, const uint32_t* idx, const float* w,
                                                 const float4* cluster_rad, int vec, uint32_t i) {
-    const V irr = jacobi_row<kFused>(cluster_rad, idx, w, starts[i], starts[i + 1], vec);
+    const V irr = jacobi_row(cluster_rad, idx, w, starts[i], starts[i + 1], vec);
     V nr = mk4(__ldg(&direct[i])) + mk4(__ldg(&albedo[i])) * irr;
     V diff = vabs(nr - mk4(rad[i]));
     irr_out[i] = f4(irr, 0.0f);
@@ -171,7 +158,7 @@ __global__ void __launch_bounds__(kJacBlock) k_jacobi(float4* direct, float4* al
     if (ctl->done) return;
     float dmax = 0.0f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float d = csr_row_update<false>(direct, albedo, irr_out, rad, starts, idx, w, cluster_rad, vec, i);
+        const float d = csr_row_update(direct, albedo, irr_out, rad, starts, idx, w, cluster_rad, vec, i);
         if (!isnan(d)) dmax = fmaxf(dmax, d);
     }
     for (int o = 16; o >= 1; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
@@ -204,7 +191,6 @@ void launch_light_surfels(cudaStream_t st, BlobRef blob, SurfelArrays s, uint32_
 // from the interleaved layout (a warp's loads are one contiguous 512-byte
 // block) and added in CSR order, exactly as k_jacobi; a lane stops at its own
 // row's length, so padding is never read. Outputs go to the original row.
-template <bool kFused>
 __device__ __forceinline__ float sell_row_update(float4* direct, float4* albedo, float4* irr_out, float4* rad,
                                                  const SellMatrix& m, const float4* crad, uint32_t sp) {
     const uint32_t row = m.perm[sp], len = m.len[sp];
@@ -217,10 +203,10 @@ __device__ __forceinline__ float sell_row_update(float4* direct, float4* albedo,
         const uint4 i1 = __ldg(reinterpret_cast<const uint4*>(ip + 128));
         const float4 w0 = __ldg(reinterpret_cast<const float4*>(wp));
         const float4 w1 = __ldg(reinterpret_cast<const float4*>(wp + 128));
-        const float4 c0 = ld_live<kFused>(&crad[i0.x]), c1 = ld_live<kFused>(&crad[i0.y]),
-                     c2 = ld_live<kFused>(&crad[i0.z]), c3 = ld_live<kFused>(&crad[i0.w]),
-                     c4 = ld_live<kFused>(&crad[i1.x]), c5 = ld_live<kFused>(&crad[i1.y]),
-                     c6 = ld_live<kFused>(&crad[i1.z]), c7 = ld_live<kFused>(&crad[i1.w]);
+        const float4 c0 = __ldg(&crad[i0.x]), c1 = __ldg(&crad[i0.y]),
+                     c2 = __ldg(&crad[i0.z]), c3 = __ldg(&crad[i0.w]),
+                     c4 = __ldg(&crad[i1.x]), c5 = __ldg(&crad[i1.y]),
+                     c6 = __ldg(&crad[i1.z]), c7 = __ldg(&crad[i1.w]);
         irr = irr + mk4(c0) * w0.x;
         irr = irr + mk4(c1) * w0.y;
         irr = irr + mk4(c2) * w0.z;
@@ -236,7 +222,7 @@ __device__ __forceinline__ float sell_row_update(float4* direct, float4* albedo,
         const uint32_t ia[4] = {i0.x, i0.y, i0.z, i0.w};
         const float wa[4] = {w0.x, w0.y, w0.z, w0.w};
         const uint32_t r4 = len - j < 4u ? len - j : 4u;
-        for (uint32_t t = 0; t < r4; ++t) irr = irr + mk4(ld_live<kFused>(&crad[ia[t]])) * wa[t];
+        for (uint32_t t = 0; t < r4; ++t) irr = irr + mk4(__ldg(&crad[ia[t]])) * wa[t];
         j += r4;
         if (j < len) {
             ip += 128;
@@ -245,7 +231,7 @@ __device__ __forceinline__ float sell_row_update(float4* direct, float4* albedo,
             const float4 w1 = __ldg(reinterpret_cast<const float4*>(wp));
             const uint32_t ib[4] = {i1.x, i1.y, i1.z, i1.w};
             const float wb[4] = {w1.x, w1.y, w1.z, w1.w};
-            for (uint32_t t = 0; t < len - j; ++t) irr = irr + mk4(ld_live<kFused>(&crad[ib[t]])) * wb[t];
+            for (uint32_t t = 0; t < len - j; ++t) irr = irr + mk4(__ldg(&crad[ib[t]])) * wb[t];
         }
     }
     V nr = mk4(__ldg(&direct[row])) + mk4(__ldg(&albedo[row])) * irr;
@@ -261,119 +247,11 @@ __global__ void __launch_bounds__(kJacBlock) k_jacobi_sell(float4* direct, float
     if (ctl->done) return;
     float dmax = 0.0f;
     for (uint32_t sp = blockIdx.x * blockDim.x + threadIdx.x; sp < n; sp += gridDim.x * blockDim.x) {
-        const float d = sell_row_update<false>(direct, albedo, irr_out, rad, m, crad, sp);
+        const float d = sell_row_update(direct, albedo, irr_out, rad, m, crad, sp);
         if (!isnan(d)) dmax = fmaxf(dmax, d);
     }
     for (int o = 16; o >= 1; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
     if ((threadIdx.x & 31) == 0 && dmax > 0.0f) atomicMax(&ctl->residual_bits, __float_as_uint(dmax));
-}
-
-// solve.rs:47-108 in ONE cooperative launch: every bounce's cluster means
-// (warp per cluster), a grid barrier, the Jacobi rows (thread per row, the
-// sliced-ELL copy when there is one) with the bounce's residual as an
-// order-free max into its own slot, a second barrier, and the stop test,
-// which every CTA evaluates on the same value. The operations and their
-// order per cluster and per row are exactly those of the per-bounce kernels,
-// so the result is bit-identical to them; what goes away is three launches
-// per bounce and the host's look at the convergence flag.
-template <bool kSell>
-__global__ void __launch_bounds__(kFusedSolveBlock) k_solve_fused(SurfelArrays s, uint32_t n, const float4* cp,
-                                                                   const uint2* crange, const uint32_t* members,
-                                                                   uint32_t nc, const uint32_t* starts,
-                                                                   const uint32_t* idx, const float* w,
-                                                                   SellMatrix m, float4* cluster_rad,
-                                                                   FusedSolve* fs, uint32_t max_bounces,
-                                                                   int no_exit, uint32_t* status, uint32_t polls) {
-    const int vec = (((uintptr_t)idx | (uintptr_t)w) & 15u) == 0 ? 1 : 0;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-    for (uint32_t it = 0; it < max_bounces; ++it) {
-        // Cluster means, a warp per cluster: 32 members' rad * area at a time,
-        // broadcast lane by lane and added in member order.
-        for (uint32_t c = gwarp; c < nc; c += nwarps) {
-            const uint2 r = crange[c];
-            V acc{0.0f, 0.0f, 0.0f};
-            for (uint32_t base = r.x; base < r.y; base += 32u) {
-                const uint32_t k = base + lane;
-                V v{0.0f, 0.0f, 0.0f};
-                if (k < r.y) {
-                    const uint32_t m = __ldg(&members[k]);
-                    const float4 rr = ld_live<true>(&s.rad[m]);
-                    const float a = __ldg(&s.p[m].w);
-                    v = V{rr.x * a, rr.y * a, rr.z * a};
-                }
-                const uint32_t cnt = r.y - base < 32u ? r.y - base : 32u;
-#pragma unroll 4
-                for (uint32_t j = 0; j < cnt; ++j)
-                    acc = acc + V{__shfl_sync(kFull, v.x, j), __shfl_sync(kFull, v.y, j), __shfl_sync(kFull, v.z, j)};
-            }
-            if (lane == 0) cluster_rad[c] = f4(acc / fmaxf(__ldg(&cp[c].w), 1e-12f), 0.0f);
-        }
-        if (!grid_barrier(&fs->bar, status, polls)) return;
-        float dmax = 0.0f;
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-            const float d = kSell ? sell_row_update<true>(s.direct, s.albedo, s.irr, s.rad, m, cluster_rad, i)
-                                  : csr_row_update<true>(s.direct, s.albedo, s.irr, s.rad, starts, idx, w,
-                                                         cluster_rad, vec, i);
-            if (!isnan(d)) dmax = fmaxf(dmax, d);
-        }
-        for (int o = 16; o >= 1; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
-        if ((threadIdx.x & 31) == 0 && dmax > 0.0f) atomicMax(&fs->residual_bits[it], __float_as_uint(dmax));
-        if (!grid_barrier(&fs->bar, status, polls)) return;
-        const uint32_t rb = __ldcg(&fs->residual_bits[it]);
-        if (lead) {
-            fs->iterations = it + 1;
-            fs->last_residual = rb;
-        }
-        if (__uint_as_float(rb) < 1e-4f && !no_exit) {  // solve.rs:96-101
-            if (lead) fs->done = 1;
-            break;
-        }
-    }
-}
-
-int fused_solve_grid(uint32_t n, uint32_t nc, bool sell) {
-    static int per_sm[2] = {-1, -1};
-    int& ps = per_sm[sell ? 1 : 0];
-    if (ps < 0) {
-        int v = 0;
-        cudaError_t e = sell ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_solve_fused<true>,
-                                                                             kFusedSolveBlock, 0)
-                             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_solve_fused<false>,
-                                                                             kFusedSolveBlock, 0);
-        ps = e == cudaSuccess ? v : 0;
-    }
-    if (ps <= 0) return 0;
-    const unsigned long long need_rows = ((unsigned long long)n + kFusedSolveBlock - 1) / kFusedSolveBlock;
-    unsigned long long need = need_rows > nc ? need_rows : nc;
-    // At most one CTA per SM: the grid barrier's cost grows with the number
-    // of CTAs arriving; rows and clusters are taken grid-stride.
-    const unsigned long long cap = (unsigned long long)sm_count();
-    if (need < 1) need = 1;
-    return (int)(need < cap ? need : cap);
-}
-
-int launch_solve_fused(cudaStream_t st, int grid, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
-                       const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
-                       const float* w, const SellMatrix* sell, float4* cluster_rad, FusedSolve* fs,
-                       uint32_t max_bounces, int no_exit, uint32_t* status, uint32_t polls) {
-    SellMatrix m = sell ? *sell : SellMatrix{};
-    void* args[] = {&s, &n, &cp, &crange, &members, &nc, &starts, &idx, &w, &m, &cluster_rad, &fs, &max_bounces,
-                    &no_exit, &status, &polls};
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3((unsigned)kFusedSolveBlock);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    const void* fn = sell ? (const void*)k_solve_fused<true> : (const void*)k_solve_fused<false>;
-    return cudaLaunchKernelExC(&cfg, fn, args) == cudaSuccess ? 1 : -1;
 }
 
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,

@@ -194,23 +194,6 @@ void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const floa
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
                          const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches,
                          int no_exit = 0, const SellMatrix* sell = nullptr);
-// The Jacobi solve in one cooperative launch (k_solve.cu): bounce state in
-// one zeroed block; residual_bits[k] collects bounce k's max change.
-static constexpr int kFusedSolveBlock = 256;
-static constexpr uint32_t kFusedSolveMaxBounces = 256;
-static constexpr uint32_t kFusedSolveMaxRows = 1u << 18;
-struct FusedSolve {
-    MsBarrier bar;
-    uint32_t iterations, last_residual, done, pad;
-    uint32_t residual_bits[kFusedSolveMaxBounces];
-};
-// Grid of the fused solve for n rows and nc clusters (0: cooperative launch
-// unavailable); launch returns 1, or -1 when the launch was refused.
-int fused_solve_grid(uint32_t n, uint32_t nc, bool sell);
-int launch_solve_fused(cudaStream_t st, int grid, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
-                       const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
-                       const float* w, const SellMatrix* sell, float4* cluster_rad, FusedSolve* fs,
-                       uint32_t max_bounces, int no_exit, uint32_t* status, uint32_t polls);
 // Sliced-ELL construction: row link counts (keys) with the identity (vals);
 // after a stable descending sort of (keys, vals), the slice sizes, then the
 // interleaved copy of idx and w.
@@ -366,6 +349,7 @@ struct MsParams {
     MsBarrier* bar;
     uint32_t* status;
     const float* srgb_t;
+    uint32_t polls;        // poll budget of each grid barrier
 };
 // Cooperative launch (every CTA resident); capturable in a CUDA graph.
 // Returns 1, or -1 if the launch was refused.

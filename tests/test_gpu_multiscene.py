@@ -108,3 +108,25 @@ def test_a_rerendered_member_is_refused(scenes):
     with pytest.raises(ifx.DeviceError):
         ms.run()
     ms.close()
+
+
+def test_grid_barrier_runs_out_and_the_packed_frame_recovers(scenes):
+    """The packed launch's grid barriers are bounded: with no polls at all
+    every CTA but the last to arrive gives up, the run returns
+    IFX_ERR_TIMEOUT (no hang, no fault), and after a rebuild with the default
+    budget the same packed frame is bit-identical to the unbatched frames."""
+    ms = ifx.MultiScene(0)
+    for d in scenes:
+        ms.add(d["ctx"], d["side"], d["side"], BOUNCES)
+    ms.set_wait_limit(0)
+    ms.build(autotune=False)
+    with pytest.raises(ifx.WaitTimeout, match="grid barrier"):
+        ms.run()
+    ms.set_wait_limit(None)
+    ms.build(autotune=False)
+    ms.run()
+    for i, d in enumerate(scenes):
+        lin, _, st = ms.download(i)
+        rl, _, rst = unbatched(d)
+        assert st.iterations == rst.iterations and lin.tobytes() == rl.tobytes(), i
+    ms.close()
