@@ -325,9 +325,11 @@ def run_ours(args, world, rank, local) -> dict | None:
     achieved = flops / (avg[dom] / 1e3) / 1e12
     traffic = None
     tj = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tj):
+    traffic_src = None
+    if os.path.exists(tj) and not args.film and not args.surfels:
         with open(tj) as f:
-            traffic = json.load(f).get(args.workload, {}).get(dom)
+            tw = json.load(f).get(args.workload, {})
+        traffic, traffic_src = tw.get(dom), tw.get("_source")
 
     # Issue-slot roofline of the same kernel: its warp instructions per launch
     # (ncu, the same workload) over the live duration, against 148 SMs x 4
@@ -336,12 +338,14 @@ def run_ours(args, world, rank, local) -> dict | None:
     ij = os.path.join(ROOT, "profiles", "ncu_issue.json")
     if os.path.exists(ij) and not args.film and not args.surfels:
         with open(ij) as f:
-            inst = json.load(f).get(args.workload, {}).get(dom)
+            iw = json.load(f).get(args.workload, {})
+        inst = iw.get(dom)
         mhz = (clocks or {}).get("sm_mhz") or peaks.get("sm_max_mhz") or 1965.0
         if inst:
             slots = N_SMS * 4 * mhz * 1e6 * (avg[dom] / 1e3)
             issue = {"warp_inst_per_launch": inst, "issue_slots_per_launch": slots, "frac": inst / slots,
-                     "sm_mhz": mhz, "source": "profiles/ncu_issue.json (ncu smsp__inst_executed.sum)"}
+                     "sm_mhz": mhz, "source": "profiles/ncu_issue.json (ncu smsp__inst_executed.sum): "
+                                              + str(iw.get("_source", ""))}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -361,7 +365,7 @@ def run_ours(args, world, rank, local) -> dict | None:
         "kernel_ms": avg,
         "surfel_generation_s": gen_s,
         "roofline": {"kernel": dom, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic,
+                     "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                      "flops_per_launch": flops, "peak_source": f"fp32 CUDA-core peak from {peak_src}",
                      "work": {k: float(v[1]) for k, v in work.items()}, "issue": issue},
         "e2e": {"value": e2e_ev_sum / (e2e_max / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,

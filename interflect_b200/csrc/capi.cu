@@ -56,7 +56,6 @@ struct ifx_ctx {
     DBuf blob;
     BlobRef blobref{};
     uint32_t stage_limit = kDefaultStageLimit;
-    bool scene_bvh = false;  // the uploaded program traverses a BVH
     bool leafgrid_on = true;  // build per-cell leaf lists for large BVHs (ifx_set_leaf_grid)
     DBuf lg_U, lg_count, lg_start, lg_leaves, lg_leaf, lg_key;
     uint32_t lg_cells = 0, lg_entries = 0;
@@ -523,14 +522,10 @@ extern "C" int ifx_timer_stop(ifx_ctx* ctx, float* ms) {
 }
 
 // Staging of the scene program for the ray-marching kernels: the whole
-// geometry prefix when it fits the limit, else (BVH scenes) the header,
-// objects and BVH nodes alone when those fit, else nothing (read through L1).
+// geometry prefix when it fits the limit, else nothing (read through L1).
 static void choose_staging(ifx_ctx* ctx) {
     BlobRef& b = ctx->blobref;
-    if (b.stage_bytes <= ctx->stage_limit) b.staged = 1;
-    else if (ctx->scene_bvh && b.part_nodes > 0 && align16(b.part_head) + b.part_nodes <= ctx->stage_limit)
-        b.staged = 2;
-    else b.staged = 0;
+    b.staged = b.stage_bytes <= ctx->stage_limit ? 1 : 0;
 }
 
 extern "C" int ifx_set_stage_limit(ifx_ctx* ctx, uint32_t max_bytes) {
@@ -654,13 +649,6 @@ extern "C" int ifx_scene_upload(ifx_ctx* ctx, const ifx_scene* scene) {
     ctx->blobref.ptr = (const uint8_t*)ctx->blob.p;
     ctx->blobref.bytes = (uint32_t)blob.size();
     ctx->blobref.stage_bytes = reinterpret_cast<const BlobHeader*>(blob.data())->off_lights;
-    {
-        const BlobHeader* bh = reinterpret_cast<const BlobHeader*>(blob.data());
-        ctx->blobref.part_head = bh->off_prims;
-        ctx->blobref.part_nodes_off = bh->off_nodes;
-        ctx->blobref.part_nodes = (uint32_t)bh->n_nodes * (uint32_t)sizeof(DNode);
-        ctx->scene_bvh = bh->use_bvh != 0;
-    }
     choose_staging(ctx);
     ctx->blobref.stack_depth = maxd + 2;
     ctx->blobref.wait_polls = ctx->wait_polls;

@@ -202,8 +202,6 @@ struct Counts {
 // kStageDrainPolls) for its copy in flight to land so that no copy writes
 // shared memory after the CTA has left, and the caller must return without
 // tracing. `bytes` is a multiple of 16 and both addresses are 16-byte aligned.
-// A second range (bytes2 > 0: gsrc2 to smem + off2, the same rules) can ride
-// on the same mbarrier.
 static constexpr uint32_t kStageDrainPolls = 1u << 22;
 __device__ __forceinline__ uint32_t mbar_try_wait(uint32_t bar) {
     uint32_t done;
@@ -225,9 +223,7 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const uint8_t* src, uint
     }
 }
 __device__ __forceinline__ bool stage_scene(const uint8_t* gblob, uint32_t bytes, uint8_t* smem,
-                                            uint64_t* mbar, uint32_t* status, uint32_t polls,
-                                            const uint8_t* gsrc2 = nullptr, uint32_t bytes2 = 0,
-                                            uint32_t off2 = 0) {
+                                            uint64_t* mbar, uint32_t* status, uint32_t polls) {
     uint32_t bar = (uint32_t)__cvta_generic_to_shared(mbar);
     uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem);
     if (threadIdx.x == 0) {
@@ -236,10 +232,8 @@ __device__ __forceinline__ bool stage_scene(const uint8_t* gblob, uint32_t bytes
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes + bytes2)
-                     : "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
         bulk_copy(dst, gblob, bytes, bar);
-        if (bytes2) bulk_copy(dst + off2, gsrc2, bytes2, bar);
     }
     uint32_t done = 0;
     for (uint32_t spin = 0; spin < polls; ++spin) {
@@ -679,6 +673,16 @@ __device__ __forceinline__ TraceHit trace(const SceneView& sv, V ro, V rd, float
     return TraceHit{false, 0.0f, V{0.0f, 0.0f, 0.0f}, 0u, steps};
 }
 
+// True when this step's cone term X = k * d / max(t - y, 1e-4)
+// (trace.rs:84-124) is provably >= res, so that res = min(res, X) leaves res
+// unchanged and X need not be formed: y = h^2 / (2 ph) < h / 2 when h < ph
+// (else y = 0), so d = sqrt(h^2 - y^2) > 0.866 h, and max(t - y, 1e-4) <=
+// max(t, 1e-4). The test uses products only, with a 1e-4 relative margin over
+// their rounding; NaN operands fail it, and X is then formed as usual.
+__device__ __forceinline__ bool cone_cannot_lower(float h, float t, float k, float res) {
+    return k * h * 0.8660f >= res * fmaxf(t, 1e-4f) * 1.0001f;
+}
+
 // trace.rs:84-124
 template <class C>
 __device__ __forceinline__ float soft_shadow(const SceneView& sv, V ro, V rd, float tmin, float tmax, float k,
@@ -695,15 +699,17 @@ __device__ __forceinline__ float soft_shadow(const SceneView& sv, V ro, V rd, fl
             steps_out = steps;
             return 0.0f;
         }
-        float y, d;
-        if (h < ph) {
-            y = h * h / (2.0f * ph);
-            d = sqrtf(fmaxf(h * h - y * y, 0.0f));
-        } else {
-            y = 0.0f;
-            d = h;
+        if (!cone_cannot_lower(h, t, k, res)) {
+            float y, d;
+            if (h < ph) {
+                y = h * h / (2.0f * ph);
+                d = sqrtf(fmaxf(h * h - y * y, 0.0f));
+            } else {
+                y = 0.0f;
+                d = h;
+            }
+            res = fminf(res, k * d / fmaxf(t - y, 1e-4f));
         }
-        res = fminf(res, k * d / fmaxf(t - y, 1e-4f));
         if (res < 1e-3f) {
             steps_out = steps;
             return 0.0f;
@@ -741,15 +747,17 @@ __device__ __forceinline__ bool shadow_step(const SceneView& sv, ShadowRay& s, f
         vis = 0.0f;
         return true;
     }
-    float y, d;
-    if (h < s.ph) {
-        y = h * h / (2.0f * s.ph);
-        d = sqrtf(fmaxf(h * h - y * y, 0.0f));
-    } else {
-        y = 0.0f;
-        d = h;
+    if (!cone_cannot_lower(h, s.t, s.k, s.res)) {
+        float y, d;
+        if (h < s.ph) {
+            y = h * h / (2.0f * s.ph);
+            d = sqrtf(fmaxf(h * h - y * y, 0.0f));
+        } else {
+            y = 0.0f;
+            d = h;
+        }
+        s.res = fminf(s.res, s.k * d / fmaxf(s.t - y, 1e-4f));
     }
-    s.res = fminf(s.res, s.k * d / fmaxf(s.t - y, 1e-4f));
     if (s.res < 1e-3f) {
         vis = 0.0f;
         return true;
@@ -890,15 +898,17 @@ __device__ __forceinline__ bool shadow_step_w(const SceneView& sv, ShadowRay& s,
         vis = 0.0f;
         return true;
     }
-    float y, d;
-    if (h < s.ph) {
-        y = h * h / (2.0f * s.ph);
-        d = sqrtf(fmaxf(h * h - y * y, 0.0f));
-    } else {
-        y = 0.0f;
-        d = h;
+    if (!cone_cannot_lower(h, s.t, s.k, s.res)) {
+        float y, d;
+        if (h < s.ph) {
+            y = h * h / (2.0f * s.ph);
+            d = sqrtf(fmaxf(h * h - y * y, 0.0f));
+        } else {
+            y = 0.0f;
+            d = h;
+        }
+        s.res = fminf(s.res, s.k * d / fmaxf(s.t - y, 1e-4f));
     }
-    s.res = fminf(s.res, s.k * d / fmaxf(s.t - y, 1e-4f));
     if (s.res < 1e-3f) {
         vis = 0.0f;
         return true;

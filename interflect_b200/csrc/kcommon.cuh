@@ -13,15 +13,13 @@ static constexpr unsigned kFull = 0xffffffffu;
 // Dynamic shared memory of a tracing CTA: the staged blob (when it fits)
 // followed by the threads' BVH stacks.
 static inline size_t blob_smem(const BlobRef& b, int block) {
-    size_t s = b.staged == 1 ? (size_t)align16(b.stage_bytes)
-                             : b.staged == 2 ? (size_t)align16(b.part_head) + b.part_nodes : 0;
+    size_t s = b.staged ? (size_t)align16(b.stage_bytes) : 0;
     return s + (size_t)b.stack_depth * (size_t)block * 8u;  // node index + box distance
 }
 
 // Stages the blob's geometry prefix into dynamic shared memory (one bulk
-// copy), or for larger scenes only its objects and BVH nodes (two copies on
-// one mbarrier), or reads it in place, and points the view at this thread's
-// stack. All threads of the CTA must call this before any of them
+// copy) or, for large scenes, reads it in place, and points the view at this
+// thread's stack. All threads of the CTA must call this before any of them
 // exits. Returns false if staging timed out.
 __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsmem, uint64_t* mbar,
                                                uint32_t* status, SceneView& sv) {
@@ -29,23 +27,13 @@ __device__ __forceinline__ bool scene_prologue(const BlobRef& blob, uint8_t* dsm
     sv.status = status;
     sv.lg = blob.lg;
     uint32_t used = 0;
-    if (blob.staged == 1) {
+    if (blob.staged) {
         if (!stage_scene(blob.ptr, blob.stage_bytes, dsmem, mbar, status, blob.wait_polls)) return false;
         const SceneView s = make_view(dsmem);
         sv.objs = s.objs;
         sv.prims = s.prims;
         sv.nodes = s.nodes;
         used = align16(blob.stage_bytes);
-    } else if (blob.staged == 2) {
-        // Header and objects, then the BVH nodes; primitives stay in global
-        // memory (read through L1).
-        const uint32_t head = align16(blob.part_head);
-        if (!stage_scene(blob.ptr, blob.part_head, dsmem, mbar, status, blob.wait_polls,
-                         blob.ptr + blob.part_nodes_off, blob.part_nodes, head))
-            return false;
-        sv.objs = reinterpret_cast<const DObject*>(dsmem + reinterpret_cast<const BlobHeader*>(dsmem)->off_objects);
-        sv.nodes = reinterpret_cast<const DNode*>(dsmem + head);
-        used = head + blob.part_nodes;
     }
     uint32_t* stk = reinterpret_cast<uint32_t*>(dsmem + used);
     sv.stk = stk + threadIdx.x;

@@ -23,9 +23,6 @@ struct BlobRef {
     int stack_depth;  // BVH traversal stack entries per thread (tree depth + 2)
     uint32_t wait_polls;  // poll budget of the staging wait (kDefaultWaitPolls unless the host lowers it)
     int tree3;            // BVH in use and made of a root and two leaves: the NoCount3 kernels apply
-    // staged == 2: only [0, part_head) (header and objects) and the BVH nodes
-    // [part_nodes_off, + part_nodes) are copied into shared memory.
-    uint32_t part_head, part_nodes_off, part_nodes;
     LeafGrid lg;          // enabled only for the scenes dist_fast serves (large BVHs)
 };
 
