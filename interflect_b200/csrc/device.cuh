@@ -380,9 +380,9 @@ __device__ __forceinline__ DistHit dist_mat(const SceneView& sv, V p, C& cnt) {
         if (d < best.d) best = DistHit{d, o.mat};
     }
     if constexpr (C::kTree3) {
-        // bvh.rs:100-150 on a root and two leaves: the same prunes and visit
-        // order as the stack traversal below (the root's own test is implied
-        // by its leaves', as in dist_mat_warp3).
+        // bvh.rs:100-150 on a root and two leaves: the same tests, prunes and
+        // visit order as the stack traversal below.
+        if (sq_ge(aabb_dist2(p, sv.node(0), cnt), best.d)) return best;
         const int r = sv.node(0).link;
         const float dl = aabb_dist2(p, sv.node(1), cnt), dr = aabb_dist2(p, sv.node(r), cnt);
         const bool lfirst = sq_lt(dl, dr);
@@ -498,12 +498,8 @@ __device__ __forceinline__ DistHit dist_mat_warp3(const SceneView& sv, V p, bool
     int next = -1, last = -1;  // leaves still to pop, in order
     float dnext = 0.0f, dlast = 0.0f;
     if (active) {
-        // The root box is the union of the two leaf boxes, so its distance is
-        // at most either leaf's (each step of aabb_dist2 is a monotone
-        // rounding): when the root is pruned both leaves are too, and the
-        // uncounted kernels go straight to the leaf tests.
-        const bool root_in = sizeof(C) == 1 || !sq_ge(aabb_dist2(p, sv.node(0), cnt), best.d);
-        if (root_in) {
+        const float d0 = aabb_dist2(p, sv.node(0), cnt);
+        if (!sq_ge(d0, best.d)) {
             const int l = 1, r = sv.node(0).link;
             const float dl = aabb_dist2(p, sv.node(l), cnt);
             const float dr = aabb_dist2(p, sv.node(r), cnt);
