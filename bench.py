@@ -650,9 +650,11 @@ def run_solve_hbm(args, world, rank, local) -> dict | None:
     if sampler:
         sampler.start()
     times, st = [], None
+    launches0 = ctx.stats()["kernel_launches"]
     for _ in range(args.steps):
         st, ms = once()
         times.append(ms)
+    launches = ctx.stats()["kernel_launches"] - launches0
     clocks = sampler.stop() if sampler else None
     rad_sell = ctx.surfels()["rad"]
     # The CSR kernel on the same matrix (caller-owned device copies).
@@ -709,7 +711,7 @@ def run_solve_hbm(args, world, rank, local) -> dict | None:
                      "peak_source": peak_src},
         "csr_kernel": {"value": bpb * st.iterations / (csr_max / 1e3) / 1e9, "unit": "GB/s",
                        "ms": csr_max, "bit_identical_to_sliced_ell": same},
-        "gpu_launches": 3 * st.iterations * args.steps,
+        "gpu_launches": int(launches),
         "clocks": clocks,
     }
 

@@ -8,7 +8,7 @@
 // (cluster, rhs) its members in member order, exactly as the single-RHS
 // kernels do, so every right-hand side is bit-identical to its own solve.
 // Per-RHS done flags freeze a right-hand side at the bounce where its own
-// residual fell below 1e-4 (solve.rs:460).
+// residual fell below 1e-4 (solve.rs:99).
 #include "kcommon.cuh"
 
 namespace ifx {
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(512) k_spmm(const float4* direct, const float4
     }
 }
 
-// solve.rs:454-462 per rhs.
+// solve.rs:93-101 per rhs.
 __global__ void k_bounce_end_batched(uint32_t R, uint32_t it, uint32_t* done, uint32_t* iterations,
                                      uint32_t* res_bits, uint32_t* last_res) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) k_multi_frame(MsParams M) {
             if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && bits) atomicMax(&M.ctl[s].residual_bits, bits);
         }
         if (!grid_barrier(M.bar, M.status, M.polls)) return;
-        // solve.rs:454-462 per scene, with each scene's own bounce cap.
+        // solve.rs:93-101 per scene, with each scene's own bounce cap.
         if (blockIdx.x == 0) {
             __shared__ uint32_t live;
             if (threadIdx.x == 0) live = 0;

@@ -3,7 +3,7 @@
 
 namespace ifx {
 
-// surfel.rs:366-393: Halton seed i (bases 2, 3, 5) across the scene bounds,
+// surfel.rs:190-211: Halton seed i (bases 2, 3, 5) across the scene bounds,
 // Newton projection onto the zero level set (at most 10 steps), then the
 // on-surface and in-bounds tests. Writes the projected point with w = 1 if
 // the seed survives, w = 0 otherwise. The Poisson-disc thinning that follows
@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(128) k_gen_project(BlobRef blob, SceneConsts s
     }
 }
 
-// surfel.rs:415-432: material albedo and normal of each accepted point.
+// surfel.rs:233-246: material albedo and normal of each accepted point.
 __global__ void __launch_bounds__(128) k_gen_finalize(BlobRef blob, const float4* pts, uint32_t n, float area,
                                                        SurfelArrays s, uint32_t* status) {
     IFX_SCENE_PROLOGUE(blob, status, sv);

@@ -119,18 +119,18 @@ def ceiling_light(half, h):
     return np.array([[-half, h, -half], [half, h, -half], [half, h, half], [-half, h, half]], np.float32)
 
 
-def test_dsl_winding_yields_positive_form_factor():  # ltc.rs:418-426
+def test_dsl_winding_yields_positive_form_factor():  # ltc.rs:156-163
     assert form_factor_at(ceiling_light(1.0, 2.0), (0, 0, 0), (0, 1, 0)) > 0.05
 
 
-def test_small_distant_light_matches_analytic_limit():  # ltc.rs:431-444
+def test_small_distant_light_matches_analytic_limit():  # ltc.rs:169-181
     half, h = 0.05, 5.0
     ff = form_factor_at(ceiling_light(half, h), (0, 0, 0), (0, 1, 0))
     expect = (2 * half) ** 2 / (math.pi * h * h)
     assert abs(ff - expect) / expect < 0.02
 
 
-def test_light_below_horizon_contributes_nothing():  # ltc.rs:448-452
+def test_light_below_horizon_contributes_nothing():  # ltc.rs:186-189
     assert form_factor_at(ceiling_light(1.0, -2.0), (0, 0, 0), (0, 1, 0)) < 1e-6
 
 
@@ -182,7 +182,7 @@ def test_transfer_matrix_is_sparse_and_well_formed():  # formfactor.rs:332-360
 
 
 # -------------------------------------------------------------- solve.rs --
-def test_no_interior_surfel_is_unlit():  # solve.rs:506-535
+def test_no_interior_surfel_is_unlit():  # solve.rs:146-174
     o, k, _, _ = closed_box_transfer()
     o.light_surfels()
     o.solve(16)
@@ -192,7 +192,7 @@ def test_no_interior_surfel_is_unlit():  # solve.rs:506-535
     assert lit.min() > lit.max() * 1e-3
 
 
-def test_solve_converges():  # solve.rs:539-557
+def test_solve_converges():  # solve.rs:179-196
     o, _, _, _ = closed_box_transfer()
     o.light_surfels()
     it, res = o.solve(64)
