@@ -40,6 +40,11 @@ const int kMaxDynSmem = 227 * 1024;
 // Geometry staged plus the largest traversal stacks must fit in that.
 const uint32_t kMaxStageLimit = 128 * 1024;
 
+// ifx_frame composes a film of at least kChunkedFilm pixels in this many row
+// chunks, each copied to the host while the next is composed.
+const uint32_t kComposeChunks = 4;
+const uint64_t kChunkedFilm = 1u << 18;
+
 }  // namespace
 
 struct ifx_ctx {
@@ -125,6 +130,8 @@ struct ifx_ctx {
     DBuf msum;
     bool mean_pending = false;
     cudaEvent_t fev[4] = {};
+    // ifx_frame: the end of each composition chunk, and of the read-back
+    cudaEvent_t cev[kComposeChunks + 1] = {};
 
     // lights: current emission per light (float4), for the relight and adjoint
     DBuf lemit;
@@ -392,6 +399,8 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     for (cudaEvent_t& ev : ctx->fev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
+    for (cudaEvent_t& ev : ctx->cev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreateWithFlags(&ctx->pinned_ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     if (ensure(ctx, ctx->shsc, 32 * 8) != IFX_OK) return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->work, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8) != IFX_OK ||
@@ -460,6 +469,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     for (cudaEvent_t ev : ctx->shev)
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : ctx->fev)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ctx->cev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
     for (cudaEvent_t ev : ctx->mev)
@@ -1918,17 +1929,46 @@ extern "C" int ifx_frame(ifx_ctx* ctx, int cluster_res, uint32_t max_bounces, co
     // Join: the composition waits for the grid, then ctx->st waits for it.
     CK(cudaEventRecord(ctx->fev[1], ctx->st));
     CK(cudaStreamWaitEvent(st2, ctx->fev[1], 0));
-    ctx->launches += (uint64_t)launch_shade(st2, P, ctx->shev, kShadeCompose);
-    if (cudaGetLastError() != cudaSuccess) return finish(fail(ctx, IFX_ERR_CUDA, "launch failed"));
-    CK(cudaEventRecord(ctx->fev[3], st2));
+    // The composition in row chunks; each chunk's pixels are copied to the
+    // host on the third stream (free again: the mean row sum is joined) while
+    // the next chunk is composed.
     const size_t px = (size_t)w * h;
+    const bool copy = out_linear || out_srgb;
+    const uint32_t chunks = copy && px >= kChunkedFilm ? kComposeChunks : 1;
+    // All chunks are queued before the first copy, so that a copy into
+    // pageable memory, which holds the host until it is done, does not hold
+    // back the launches.
+    auto chunk_at = [&](uint32_t c) { return (uint32_t)((uint64_t)h * c / chunks) * w; };
+    CK(cudaEventRecord(ctx->shev[12], st2));
+    for (uint32_t c = 0; c < chunks; ++c) {
+        P.pix0 = chunk_at(c);
+        P.pix1 = chunk_at(c + 1);
+        ctx->launches += (uint64_t)launch_shade(st2, P, nullptr, kShadeCompose);
+        if (copy) CK(cudaEventRecord(ctx->cev[c], st2));
+    }
+    if (cudaGetLastError() != cudaSuccess) return finish(fail(ctx, IFX_ERR_CUDA, "launch failed"));
+    CK(cudaEventRecord(ctx->shev[13], st2));
+    CK(cudaEventRecord(ctx->fev[3], st2));
+    for (uint32_t c = 0; copy && c < chunks; ++c) {
+        const size_t p0 = chunk_at(c), n = (size_t)chunk_at(c + 1) - p0;
+        CK(cudaStreamWaitEvent(ctx->st3, ctx->cev[c], 0));
+        if (out_linear)
+            CK(cudaMemcpyAsync(out_linear + p0 * 3, (const float*)ctx->film.p + p0 * 3, n * 12,
+                               cudaMemcpyDeviceToHost, ctx->st3));
+        if (out_srgb)
+            CK(cudaMemcpyAsync(out_srgb + p0 * 3, (const uint8_t*)ctx->out8.p + p0 * 3, n * 3,
+                               cudaMemcpyDeviceToHost, ctx->st3));
+    }
     unsigned long long e = 0;
     uint32_t status = 0;
     CK(cudaMemcpyAsync(&e, &sc[16], 8, cudaMemcpyDeviceToHost, st2));
     CK(cudaMemcpyAsync(&status, P.status, 4, cudaMemcpyDeviceToHost, st2));
-    if (out_linear) CK(cudaMemcpyAsync(out_linear, ctx->film.p, px * 12, cudaMemcpyDeviceToHost, st2));
-    if (out_srgb) CK(cudaMemcpyAsync(out_srgb, ctx->out8.p, px * 3, cudaMemcpyDeviceToHost, st2));
     CK(cudaStreamWaitEvent(ctx->st, ctx->fev[3], 0));
+    if (copy) {
+        CK(cudaEventRecord(ctx->cev[kComposeChunks], ctx->st3));
+        CK(cudaStreamWaitEvent(ctx->st, ctx->cev[kComposeChunks], 0));
+        CK(cudaStreamSynchronize(ctx->st3));
+    }
     CK(cudaStreamSynchronize(st2));
     if (status) {
         CK(cudaMemsetAsync(P.status, 0, 4, ctx->st));

@@ -267,9 +267,9 @@ __global__ void __launch_bounds__(128) k_compose(ShadeParams P) {
     __shared__ float t8[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) t8[i] = P.srgb_t[i];
     __syncthreads();
-    const uint32_t total = P.w * P.h;
+    const uint32_t end = P.pix1 ? P.pix1 : P.w * P.h;
     const GatherView g = gview(P.grid);
-    for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < total; pix += gridDim.x * blockDim.x)
+    for (uint32_t pix = P.pix0 + blockIdx.x * blockDim.x + threadIdx.x; pix < end; pix += gridDim.x * blockDim.x)
         compose_pixel(sv, P, t8, g, pix, cnt);
     if constexpr (sizeof(C) > 1) cnt.flush(P.counts);
 }
@@ -317,7 +317,8 @@ static void launch_all(cudaStream_t st, const ShadeParams& p, cudaEvent_t* ev, i
     }
     if (part & kShadeCompose) {
         rec(12);
-        k_compose<C><<<grid_for(px, 128, 16), 128, sm, st>>>(with(4));
+        const unsigned long long cpx = p.pix1 ? (unsigned long long)(p.pix1 - p.pix0) : px;
+        k_compose<C><<<grid_for(cpx, 128, 16), 128, sm, st>>>(with(4));
         rec(13);
     }
 }

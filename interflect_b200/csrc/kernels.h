@@ -246,6 +246,8 @@ struct ShadeParams {
     // Re-composition over stored hits (differentiable forward): emitter
     // pixels are rewritten from the current emissions as well.
     int recompose;
+    // k_compose's pixels: [pix0, pix1), or the whole film when pix1 == 0.
+    uint32_t pix0, pix1;
 };
 // Returns the number of kernels launched. `ev` (nullable) holds
 // kShadeEvents events recorded around the kernels (see k_shade.cu);
