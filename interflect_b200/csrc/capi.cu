@@ -128,6 +128,11 @@ struct ifx_ctx {
     cudaStream_t st3 = nullptr;
     cudaEvent_t mev[2] = {};
     DBuf msum;
+    // ifx_frame's light stage and grid build beside the transfer build: the
+    // light stage's evaluation counter, the grid sort's temporary storage, and
+    // events (fork, light start, light end = grid start, grid end)
+    DBuf lsmall, cub_tmp3;
+    cudaEvent_t lev[4] = {};
     bool mean_pending = false;
     cudaEvent_t fev[4] = {};
     // ifx_frame: the end of each composition chunk, and of the read-back
@@ -253,19 +258,19 @@ static int check_status(ifx_ctx* ctx) {
 }
 
 template <class F>
-static int cub_call(ifx_ctx* ctx, F f) {
+static int cub_call(ifx_ctx* ctx, F f, DBuf& tmp) {
     size_t bytes = 0;
     CK(f(nullptr, bytes));
-    ENSURE(ctx->cub_tmp, bytes);
-    size_t have = ctx->cub_tmp.cap;
-    CK(f(ctx->cub_tmp.p, have));
+    ENSURE(tmp, bytes);
+    size_t have = tmp.cap;
+    CK(f(tmp.p, have));
     ctx->launches += 2;
     return IFX_OK;
 }
 
 #define CUB(expr)                             \
     do {                                      \
-        int r_ = cub_call(ctx, expr);         \
+        int r_ = cub_call(ctx, expr, ctx->cub_tmp); \
         if (r_ != IFX_OK) return r_;          \
     } while (0)
 
@@ -406,6 +411,8 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
     for (cudaEvent_t& ev : ctx->cev)
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
+    for (cudaEvent_t& ev : ctx->lev)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreateWithFlags(&ctx->pinned_ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     if (ensure(ctx, ctx->shsc, 32 * 8) != IFX_OK) return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->work, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8) != IFX_OK ||
@@ -414,6 +421,7 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
     if (ensure(ctx, ctx->qcur, 16 * 8) != IFX_OK || ensure(ctx, ctx->qlen, 16) != IFX_OK)
         return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->status, 16) != IFX_OK || ensure(ctx, ctx->small, 64) != IFX_OK ||
+        ensure(ctx, ctx->lsmall, 16) != IFX_OK ||
         ensure(ctx, ctx->msum, 16) != IFX_OK ||
         ensure(ctx, ctx->srgb_t, 256 * sizeof(float)) != IFX_OK || ensure(ctx, ctx->ctl, sizeof(SolveCtl)) != IFX_OK)
         return bail(cudaErrorMemoryAllocation);
@@ -454,7 +462,7 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
                     &ctx->qlen, &ctx->row_links,
                     &ctx->row_scale, &ctx->row_sum, &ctx->row_sky, &ctx->row_evals, &ctx->starts, &ctx->idx,
                     &ctx->w, &ctx->cluster_rad, &ctx->ctl, &ctx->gkeys, &ctx->gkeys_alt, &ctx->gstarts, &ctx->gp,
-                    &ctx->gn, &ctx->girr, &ctx->gitems, &ctx->film, &ctx->out8, &ctx->cub_tmp, &ctx->small,
+                    &ctx->gn, &ctx->girr, &ctx->gitems, &ctx->film, &ctx->out8, &ctx->cub_tmp, &ctx->cub_tmp3, &ctx->small, &ctx->lsmall,
                     &ctx->gen_cand, &ctx->gen_keep, &ctx->gen_off, &ctx->gen_head, &ctx->gen_pts,
                     &ctx->gen_next, &ctx->gen_state, &ctx->gen_out, &ctx->work, &ctx->bE, &ctx->bdirect, &ctx->brad, &ctx->birr, &ctx->bcrad,
                     &ctx->bdone, &ctx->biters, &ctx->bres, &ctx->blast, &ctx->bunpack, &ctx->lemit,
@@ -476,6 +484,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     for (cudaEvent_t ev : ctx->fev)
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : ctx->cev)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ctx->lev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
     for (cudaEvent_t ev : ctx->mev)
@@ -1331,14 +1341,15 @@ extern "C" int ifx_transfer_upload(ifx_ctx* ctx, const uint32_t* starts, uint64_
 // the GPU idle: there each surfel's marches run as one independent thread
 // (latency-bound, so warp-synchronous rounds would only add waiting); many
 // slots go through a queue to the lane-refilling shadow kernel.
-static int light_surfels_run(ifx_ctx* ctx, unsigned long long* evals_dev, unsigned long long* counts, float* terms) {
+// The light stage on stream st, its errors in *status.
+static int light_surfels_run(ifx_ctx* ctx, cudaStream_t st, uint32_t* status, unsigned long long* evals_dev,
+                             unsigned long long* counts, float* terms) {
     const uint32_t n = ctx->n;
     if (n == 0) return IFX_OK;
     const int nl = (int)(ctx->scene.lights.size() + ctx->scene.sphere_lights.size());
     const size_t slots = (size_t)n * (size_t)(nl > 0 ? nl : 1);
     if (slots < kLightSlotsQueued) {
-        launch_light_surfels(ctx->st, ctx->blobref, ctx->sarr(), n, evals_dev, (uint32_t*)ctx->status.p, counts,
-                             terms);
+        launch_light_surfels(st, ctx->blobref, ctx->sarr(), n, evals_dev, status, counts, terms);
         ctx->launches++;
         CKL();
         return IFX_OK;
@@ -1349,15 +1360,15 @@ static int light_surfels_run(ifx_ctx* ctx, unsigned long long* evals_dev, unsign
     ENSURE(ctx->lsc, 32);
     ShadeParams P{};
     P.blob = ctx->blobref;
-    P.status = (uint32_t*)ctx->status.p;
+    P.status = status;
     P.nl = nl;
     P.evals = evals_dev;
     P.counts = counts;
     P.q1 = (uint32_t*)ctx->lq.p;
     P.qlen = (uint32_t*)ctx->lsc.p;  // words 0..3
     unsigned long long* cursor = (unsigned long long*)ctx->lsc.p + 2;
-    CK(cudaMemsetAsync(ctx->lsc.p, 0, 32, ctx->st));
-    ctx->launches += (uint64_t)launch_light_slots(ctx->st, P, ctx->sarr(), n, (float*)ctx->lff.p,
+    CK(cudaMemsetAsync(ctx->lsc.p, 0, 32, st));
+    ctx->launches += (uint64_t)launch_light_slots(st, P, ctx->sarr(), n, (float*)ctx->lff.p,
                                                   (float*)ctx->lvis.p, terms, cursor);
     CKL();
     return IFX_OK;
@@ -1370,7 +1381,7 @@ extern "C" int ifx_light_surfels(ifx_ctx* ctx, uint64_t* evals) {
     unsigned long long* small = (unsigned long long*)ctx->small.p;
     CK(cudaMemsetAsync(small, 0, 8, ctx->st));
     CK(cudaEventRecord(ctx->ev0, ctx->st));
-    int r0 = light_surfels_run(ctx, small, ctx->work_of(IFX_KERNEL_LIGHT), nullptr);
+    int r0 = light_surfels_run(ctx, ctx->st, (uint32_t*)ctx->status.p, small, ctx->work_of(IFX_KERNEL_LIGHT), nullptr);
     if (r0) return r0;
     CK(cudaEventRecord(ctx->ev1, ctx->st));
     unsigned long long e = 0;
@@ -1622,13 +1633,13 @@ extern "C" int ifx_autotune_batched(ifx_ctx* ctx, uint32_t R, const float* E, in
 }
 
 // --------------------------------------------------------------- shade ---
-extern "C" int ifx_grid_build(ifx_ctx* ctx, float radius) {
-    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
-    CK(cudaSetDevice(ctx->device));
+// Enqueues the gather grid's build (surfel.rs:72-79, 127-140) on st, its sort
+// using the temporary buffer tmp: cell keys, the sorted items and per cell
+// their first item, and the items' positions, normals and irradiance.
+static int grid_build_on(ifx_ctx* ctx, cudaStream_t st, DBuf& tmp, float radius) {
     const HScene& s = ctx->scene;
     if (!(radius > 0.0f)) radius = (ctx->sc.diag / std::sqrt((float)s.cfg.surfels)) * 2.6f;  // main.rs:473
     GridParams g{};
-    // surfel.rs:72-79
     g.inv_cell = 1.0f / radius;
     for (int a = 0; a < 3; ++a) {
         float e = std::ceil((ctx->sc.hi[a] - ctx->sc.lo[a]) * g.inv_cell);
@@ -1639,7 +1650,6 @@ extern "C" int ifx_grid_build(ifx_ctx* ctx, float radius) {
     g.radius = radius;
     const uint32_t n = ctx->n;
     const uint32_t ncells = (uint32_t)g.dim[0] * (uint32_t)g.dim[1] * (uint32_t)g.dim[2];
-    CK(cudaEventRecord(ctx->ev0, ctx->st));
     ENSURE(ctx->gkeys, (size_t)n * 8);
     ENSURE(ctx->gkeys_alt, (size_t)n * 8);
     ENSURE(ctx->gstarts, ((size_t)ncells + 1) * 4);
@@ -1650,33 +1660,43 @@ extern "C" int ifx_grid_build(ifx_ctx* ctx, float radius) {
     auto* kin = (unsigned long long*)ctx->gkeys.p;
     auto* kout = (unsigned long long*)ctx->gkeys_alt.p;
     if (n) {
-        launch_grid_keys(ctx->st, (const float4*)ctx->sp.p, n, g, kin);
+        launch_grid_keys(st, (const float4*)ctx->sp.p, n, g, kin);
         ctx->launches++;
         CKL();
         int end_bit = 32;
         while (end_bit < 64 && (1ull << (end_bit - 32)) < (unsigned long long)ncells) ++end_bit;
-        CUB([&](void* t, size_t& b) {
-            return cub::DeviceRadixSort::SortKeys(t, b, kin, kout, (int)n, 0, end_bit, ctx->st);
-        });
+        int r = cub_call(
+            ctx, [&](void* t, size_t& b) { return cub::DeviceRadixSort::SortKeys(t, b, kin, kout, (int)n, 0, end_bit, st); },
+            tmp);
+        if (r) return r;
     }
-    launch_grid_starts(ctx->st, kout, n, ncells, (uint32_t*)ctx->gstarts.p);
+    launch_grid_starts(st, kout, n, ncells, (uint32_t*)ctx->gstarts.p);
     ctx->launches++;
     CKL();
     if (n) {
-        launch_grid_scatter(ctx->st, kout, n, ctx->sarr(), (float4*)ctx->gp.p, (float4*)ctx->gn.p,
-                            (float4*)ctx->girr.p, (uint32_t*)ctx->gitems.p);
+        launch_grid_scatter(st, kout, n, ctx->sarr(), (float4*)ctx->gp.p, (float4*)ctx->gn.p, (float4*)ctx->girr.p,
+                            (uint32_t*)ctx->gitems.p);
         ctx->launches++;
         CKL();
     }
-    CK(cudaEventRecord(ctx->ev1, ctx->st));
-    CK(cudaEventSynchronize(ctx->ev1));
-    CK(cudaEventElapsedTime(&ctx->stats.ms_grid, ctx->ev0, ctx->ev1));
     g.gp = (const float4*)ctx->gp.p;
     g.gn = (const float4*)ctx->gn.p;
     g.girr = (const float4*)ctx->girr.p;
     g.starts = (const uint32_t*)ctx->gstarts.p;
     ctx->grid = g;
     ctx->ncells = ncells;
+    return IFX_OK;
+}
+
+extern "C" int ifx_grid_build(ifx_ctx* ctx, float radius) {
+    if (!ctx || !ctx->has_scene) return fail(ctx, IFX_ERR_INVALID, "no scene uploaded");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    int r = grid_build_on(ctx, ctx->st, ctx->cub_tmp, radius);
+    if (r) return r;
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ctx->stats.ms_grid, ctx->ev0, ctx->ev1));
     ctx->has_grid = true;
     frame_changed(ctx);
     return IFX_OK;
@@ -1913,6 +1933,7 @@ extern "C" int ifx_frame(ifx_ctx* ctx, int cluster_res, uint32_t max_bounces, co
     // before this call returns.
     auto finish = [&](int code) {
         cudaStreamSynchronize(st2);
+        cudaStreamSynchronize(ctx->st3);
         if (ctx->mean_pending) {
             cudaStreamSynchronize(ctx->st3);
             cudaStreamWaitEvent(ctx->st, ctx->mev[1], 0);
@@ -1924,10 +1945,39 @@ extern "C" int ifx_frame(ifx_ctx* ctx, int cluster_res, uint32_t max_bounces, co
     if (needs_gi) {
         // The mean row sum stays on its own stream through the light stage,
         // the solve and the grid build; it is joined before the composition.
+        // The light stage and the grid's sort read only the scene and the
+        // surfels: they run on the third stream beside the transfer build (the
+        // light stage with its own evaluation counter and status word, the sort
+        // with its own temporary storage), and the solve waits for them. The
+        // grid's irradiance is refreshed after the solve.
+        unsigned long long* lsmall = (unsigned long long*)ctx->lsmall.p;
+        uint32_t* lstatus = (uint32_t*)ctx->status.p + 2;
+        CK(cudaEventRecord(ctx->lev[0], ctx->st));
+        CK(cudaStreamWaitEvent(ctx->st3, ctx->lev[0], 0));
+        CK(cudaMemsetAsync(lsmall, 0, 8, ctx->st3));
+        CK(cudaMemsetAsync(lstatus, 0, 4, ctx->st3));
+        CK(cudaEventRecord(ctx->lev[1], ctx->st3));
+        if ((r = light_surfels_run(ctx, ctx->st3, lstatus, lsmall, ctx->work_of(IFX_KERNEL_LIGHT), nullptr)))
+            return finish(r);
+        CK(cudaEventRecord(ctx->lev[2], ctx->st3));
+        if ((r = grid_build_on(ctx, ctx->st3, ctx->cub_tmp3, 0.0f))) return finish(r);
+        CK(cudaEventRecord(ctx->lev[3], ctx->st3));
         if ((r = transfer_build(ctx, cluster_res, &info.transfer, true))) return finish(r);
-        if ((r = ifx_light_surfels(ctx, &info.light_evals))) return finish(r);
+        CK(cudaStreamWaitEvent(ctx->st, ctx->lev[3], 0));
+        unsigned long long le = 0;
+        uint32_t ls = 0;
+        CK(cudaMemcpyAsync(&le, lsmall, 8, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(&ls, lstatus, 4, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (ls) return finish(status_error(ctx, ls));
+        CK(cudaEventElapsedTime(&ctx->stats.ms_light, ctx->lev[1], ctx->lev[2]));
+        CK(cudaEventElapsedTime(&ctx->stats.ms_grid, ctx->lev[2], ctx->lev[3]));
+        info.light_evals = le;
         if ((r = ifx_solve(ctx, max_bounces, &info.solve))) return finish(r);
-        if ((r = ifx_grid_build(ctx, 0.0f))) return finish(r);
+        ctx->launches += (uint64_t)launch_grid_refresh(ctx->st, (const uint32_t*)ctx->gitems.p, ctx->sarr().irr,
+                                                       ctx->n, (float4*)ctx->girr.p);
+        CKL();
+        ctx->has_grid = true;
         if ((r = join_mean(ctx))) return finish(r);
         P.grid = ctx->grid;
     }
@@ -2057,7 +2107,7 @@ extern "C" int ifx_diff_setup(ifx_ctx* ctx, const ifx_camera* cam, uint32_t w, u
     // 1. Each surfel's light factors (with direct = rad = E as a side effect).
     ENSURE(ctx->dterms, (size_t)n * (nl ? nl : 1) * 4);
     unsigned long long* small = (unsigned long long*)ctx->small.p;
-    int r = light_surfels_run(ctx, small, nullptr, (float*)ctx->dterms.p);
+    int r = light_surfels_run(ctx, ctx->st, (uint32_t*)ctx->status.p, small, nullptr, (float*)ctx->dterms.p);
     if (r) return r;
     r = check_status(ctx);
     if (r) return r;
@@ -2373,7 +2423,9 @@ extern "C" int ifx_multiscene_add(ifx_multiscene* ms, ifx_ctx* ctx, const ifx_ca
     if (cudaSetDevice(ctx->device) != cudaSuccess) return msfail(ms, IFX_ERR_CUDA, "cudaSetDevice failed");
     const uint32_t n = ctx->n, nl = ctx->nl;
     int r = ensure(ctx, ctx->dterms, (size_t)n * (nl ? nl : 1) * 4);
-    if (!r) r = light_surfels_run(ctx, (unsigned long long*)ctx->small.p, nullptr, (float*)ctx->dterms.p);
+    if (!r)
+        r = light_surfels_run(ctx, ctx->st, (uint32_t*)ctx->status.p, (unsigned long long*)ctx->small.p, nullptr,
+                              (float*)ctx->dterms.p);
     if (!r) r = check_status(ctx);
     if (!r) r = ifx_grid_build(ctx, 0.0f);
     ShadeParams P{};
