@@ -133,6 +133,8 @@ struct ifx_ctx {
     // events (fork, light start, light end = grid start, grid end)
     DBuf lsmall, cub_tmp3;
     cudaEvent_t lev[4] = {};
+    // transfer build: the closure's queue ready, the closure done (third stream)
+    cudaEvent_t tev[2] = {};
     bool mean_pending = false;
     cudaEvent_t fev[4] = {};
     // ifx_frame: the end of each composition chunk, and of the read-back
@@ -413,6 +415,8 @@ extern "C" int ifx_ctx_create(int device, ifx_ctx** out) {
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     for (cudaEvent_t& ev : ctx->lev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
+    for (cudaEvent_t& ev : ctx->tev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreateWithFlags(&ctx->pinned_ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     if (ensure(ctx, ctx->shsc, 32 * 8) != IFX_OK) return bail(cudaErrorMemoryAllocation);
     if (ensure(ctx, ctx->work, IFX_NUM_KERNELS * IFX_WORK_COUNTERS * 8) != IFX_OK ||
@@ -486,6 +490,8 @@ extern "C" void ifx_ctx_destroy(ifx_ctx* ctx) {
     for (cudaEvent_t ev : ctx->cev)
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : ctx->lev)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ctx->tev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->pinned_ev) cudaEventDestroy(ctx->pinned_ev);
     for (cudaEvent_t ev : ctx->mev)
@@ -1104,6 +1110,21 @@ static int transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out,
         });
         corder = vout;
     }
+    // The hemisphere closure (trace.rs:165-199) needs only the surfels and its
+    // queue order: it runs on the third stream while the visibility queue is
+    // sorted and marched here, and the rows wait for it. Cursors start at zero.
+    ENSURE(ctx->clo, (size_t)n * 16 * 2);
+    unsigned long long* cur = (unsigned long long*)ctx->qcur.p;
+    CK(cudaMemsetAsync(cur, 0, 16 * 8, ctx->st));
+    CK(cudaEventRecord(ctx->tev[0], ctx->st));
+    CK(cudaStreamWaitEvent(ctx->st3, ctx->tev[0], 0));
+    CK(cudaEventRecord(ctx->kc0, ctx->st3));
+    launch_closure(ctx->st3, ctx->blobref, ctx->sc, sp, sn, n, corder, (uint16_t*)ctx->clo.p, status,
+                   ctx->work_of(IFX_KERNEL_CLOSURE), &cur[1]);
+    ctx->launches++;
+    CKL();
+    CK(cudaEventRecord(ctx->kc1, ctx->st3));
+    CK(cudaEventRecord(ctx->tev[1], ctx->st3));
     const uint32_t* vorder = nullptr;
     if (ncand > 1 && ncand <= 0x7fffffffull) {
         ENSURE(ctx->vkey, ncand * 8);
@@ -1123,10 +1144,7 @@ static int transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out,
         });
         vorder = vout;
     }
-    // Visibility and closure (persistent kernels; cursors start at zero).
-    ENSURE(ctx->clo, (size_t)n * 16 * 2);
-    unsigned long long* cur = (unsigned long long*)ctx->qcur.p;
-    CK(cudaMemsetAsync(cur, 0, 16 * 8, ctx->st));
+    // Visibility (a persistent kernel).
     CK(cudaEventRecord(ctx->kv0, ctx->st));
     launch_visibility(ctx->st, ctx->blobref, ctx->sc, sp, sn, cp, cn, (const uint32_t*)ctx->cand_c.p,
                       (const uint32_t*)ctx->cand_row.p, vorder, ncand, (float*)ctx->cand_vis.p,
@@ -1134,12 +1152,7 @@ static int transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out,
     if (ncand) ctx->launches++;
     CKL();
     CK(cudaEventRecord(ctx->kv1, ctx->st));
-    CK(cudaEventRecord(ctx->kc0, ctx->st));
-    launch_closure(ctx->st, ctx->blobref, ctx->sc, sp, sn, n, corder, (uint16_t*)ctx->clo.p, status,
-                   ctx->work_of(IFX_KERNEL_CLOSURE), &cur[1]);
-    ctx->launches++;
-    CKL();
-    CK(cudaEventRecord(ctx->kc1, ctx->st));
+    CK(cudaStreamWaitEvent(ctx->st, ctx->tev[1], 0));
 
     // Rows: links, ordered sums, calibration, CSR.
     ENSURE(ctx->row_links, ((size_t)n + 1) * 4);
@@ -1228,7 +1241,11 @@ static int transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out,
 }
 
 extern "C" int ifx_transfer_build(ifx_ctx* ctx, int cluster_res, ifx_transfer_info* out) {
-    return transfer_build(ctx, cluster_res, out, false);
+    const int r = transfer_build(ctx, cluster_res, out, false);
+    // A build that failed part way may have left the closure on the third
+    // stream: nothing of it stays in flight once the call returns.
+    if (r && ctx) cudaStreamSynchronize(ctx->st3);
+    return r;
 }
 
 // Joins a deferred mean row sum in stream order: ctx->st (and whatever later
