@@ -16,8 +16,11 @@
  *  - Vectors are packed f32 triples (x, y, z) in caller-owned host memory.
  *    Output pointers documented as nullable may be NULL to skip that copy.
  *  - Device state (scene, surfels, transfer matrix, grid, film) is owned by
- *    the context. A context drives one GPU on one CUDA stream; it is not
- *    thread-safe, but separate contexts are independent.
+ *    the context. A context drives one GPU from its own CUDA streams, idle
+ *    when a call returns (ifx_surfels_upload has read the caller's arrays
+ *    when it returns; its copies to the device stay queued ahead of every
+ *    later call); it is not thread-safe, but separate contexts are
+ *    independent.
  *  - There is no CPU fallback: without a usable CUDA device every
  *    device-side call fails with IFX_ERR_CUDA.
  *  - Results are deterministic: bit-identical across runs and launch
@@ -325,8 +328,11 @@ int ifx_render_frame(ifx_ctx* ctx, const ifx_camera* cam, int mode, uint32_t w, 
  * ifx_grid_build(0), then ifx_render_frame(cam, mode, ...), with results
  * identical to those calls made in that order. The shading passes that read
  * no GI data (primary hits, their shadow rays, mirror rays and theirs) run
- * on a second CUDA stream while the GI stages run; only the composition
- * waits for the grid. Other modes skip the GI stages, as main.rs does. */
+ * on a second CUDA stream while the GI stages run, and the light stage, the
+ * grid's sort and the transfer's hemisphere closure on a third beside the
+ * transfer build; only the composition waits for the grid, and a large
+ * film is copied out in row chunks while the rest is composed. Other modes
+ * skip the GI stages, as main.rs does. */
 typedef struct ifx_frame_info {
     ifx_transfer_info transfer; /* as ifx_transfer_build reports it */
     uint64_t light_evals;       /* ifx_light_surfels */
