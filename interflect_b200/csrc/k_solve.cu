@@ -8,6 +8,14 @@
 
 namespace ifx {
 
+// Programmatic dependent launch between the bounce kernels: a kernel starts
+// by waiting until the previous kernel in its stream has completed and its
+// writes are visible (pdl_wait), and once its main loop is done it lets the
+// next kernel be scheduled (pdl_trigger), whose CTAs then wait in their own
+// pdl_wait. Both are no-ops in a launch without the programmatic attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long* out) {
     for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(out, v);
@@ -95,10 +103,12 @@ static constexpr int kAggBlock = 128;
 __global__ void __launch_bounds__(kAggBlock) k_cluster_agg(const float4* rad, const float4* sp, const float4* cp,
                                                             const uint2* crange, const uint32_t* members,
                                                             uint32_t nc, float4* cluster_rad, const SolveCtl* ctl) {
+    pdl_wait();
     if (ctl->done) return;
     __shared__ float4 buf[2][kAggBlock];
     for (uint32_t c = blockIdx.x; c < nc; c += gridDim.x)
         cluster_mean<kAggBlock>(rad, sp, cp, crange, members, c, cluster_rad, buf);
+    pdl_trigger();
 }
 
 // solve.rs:76-102: one Jacobi row per thread, its links added in CSR order
@@ -155,18 +165,22 @@ __global__ void __launch_bounds__(kJacBlock) k_jacobi(float4* direct, float4* al
                                                        uint32_t n, const uint32_t* starts, const uint32_t* idx,
                                                        const float* w, const float4* cluster_rad, SolveCtl* ctl,
                                                        int vec) {
+    pdl_wait();
     if (ctl->done) return;
     float dmax = 0.0f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float d = csr_row_update(direct, albedo, irr_out, rad, starts, idx, w, cluster_rad, vec, i);
         if (!isnan(d)) dmax = fmaxf(dmax, d);
     }
+    pdl_trigger();
     for (int o = 16; o >= 1; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
     if ((threadIdx.x & 31) == 0 && dmax > 0.0f) atomicMax(&ctl->residual_bits, __float_as_uint(dmax));
 }
 
 // solve.rs:454-462; no_exit keeps every bounce running (fixed bounce count).
 __global__ void k_bounce_end(SolveCtl* ctl, uint32_t it, int no_exit) {
+    pdl_wait();
+    pdl_trigger();
     if (ctl->done) return;
     float res = __uint_as_float(ctl->residual_bits);
     ctl->iterations = it + 1;
@@ -244,31 +258,51 @@ __device__ __forceinline__ float sell_row_update(float4* direct, float4* albedo,
 __global__ void __launch_bounds__(kJacBlock) k_jacobi_sell(float4* direct, float4* albedo, float4* irr_out,
                                                             float4* rad, uint32_t n, SellMatrix m,
                                                             const float4* __restrict__ crad, SolveCtl* ctl) {
+    pdl_wait();
     if (ctl->done) return;
     float dmax = 0.0f;
     for (uint32_t sp = blockIdx.x * blockDim.x + threadIdx.x; sp < n; sp += gridDim.x * blockDim.x) {
         const float d = sell_row_update(direct, albedo, irr_out, rad, m, crad, sp);
         if (!isnan(d)) dmax = fmaxf(dmax, d);
     }
+    pdl_trigger();
     for (int o = 16; o >= 1; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
     if ((threadIdx.x & 31) == 0 && dmax > 0.0f) atomicMax(&ctl->residual_bits, __float_as_uint(dmax));
+}
+
+// A bounce kernel launched with the programmatic-serialization attribute:
+// the stream (or the captured graph's edge) lets it start once the previous
+// kernel has triggered, and pdl_wait orders its work after that kernel.
+template <typename... K, typename... A>
+static void launch_pdl(void (*kernel)(K...), unsigned grid, unsigned block, cudaStream_t st, A... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 void launch_solve_bounce(cudaStream_t st, SurfelArrays s, uint32_t n, const float4* cp, const uint2* crange,
                          const uint32_t* members, uint32_t nc, const uint32_t* starts, const uint32_t* idx,
                          const float* w, float4* cluster_rad, SolveCtl* ctl, uint32_t it, int* launches,
                          int no_exit, const SellMatrix* sell) {
-    k_cluster_agg<<<nc < 4096u ? nc : 4096u, kAggBlock, 0, st>>>(s.rad, s.p, cp, crange, members, nc, cluster_rad,
-                                                                   ctl);
+    launch_pdl(k_cluster_agg, nc < 4096u ? nc : 4096u, kAggBlock, st, (const float4*)s.rad, (const float4*)s.p, cp,
+               crange, members, nc, cluster_rad, (const SolveCtl*)ctl);
     if (sell && sell->perm) {
-        k_jacobi_sell<<<grid_for(n, kJacBlock), kJacBlock, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, *sell,
-                                                                   cluster_rad, ctl);
+        launch_pdl(k_jacobi_sell, grid_for(n, kJacBlock), kJacBlock, st, s.direct, s.albedo, s.irr, s.rad, n, *sell,
+                   (const float4*)cluster_rad, ctl);
     } else {
         const int vec = (((uintptr_t)idx | (uintptr_t)w) & 15u) == 0 ? 1 : 0;
-        k_jacobi<<<grid_for(n, kJacBlock), kJacBlock, 0, st>>>(s.direct, s.albedo, s.irr, s.rad, n, starts, idx, w,
-                                                              cluster_rad, ctl, vec);
+        launch_pdl(k_jacobi, grid_for(n, kJacBlock), kJacBlock, st, s.direct, s.albedo, s.irr, s.rad, n, starts, idx,
+                   w, (const float4*)cluster_rad, ctl, vec);
     }
-    k_bounce_end<<<1, 1, 0, st>>>(ctl, it, no_exit);
+    launch_pdl(k_bounce_end, 1u, 1u, st, ctl, it, no_exit);
     *launches += 3;
 }
 
